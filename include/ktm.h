@@ -1,0 +1,174 @@
+/*
+ * ktm.h -- C ABI of libktm.so, a B200 (sm_100a) prestack Kirchhoff time
+ * migration (PSTM) library that is a drop-in for the psktmCPU.c /
+ * psktmFunctions.c path of wjb19/seismic-migration.
+ *
+ * Conventions shared by every entry point
+ *   - Image layout: float[Nx][Ny][Nz], tau fastest (psktmCPU.c:84), where the
+ *     Z axis is ONE-WAY time tau in seconds: the traveltime of a zero-offset
+ *     pair is 2*tau (psktmCPU.c:46, :78-79).
+ *   - Trace layout: float[traceNo][tracePts], trace-contiguous
+ *     (psktmCPU.c:85 reads traces[it + k*tracePts]).
+ *   - Coordinates: midpoint and HALF-offset vectors, source = mid - off,
+ *     receiver = mid + off (ktmConvertXYtoOffMid.m:12, psktmCPU.c:65-72).
+ *   - "slowness" in the reference signature is a velocity v(tau) in m/s,
+ *     one value per tau sample (psktmCPU.c:48 squares and inverts it).
+ *   - Every int-returning entry point returns KTM_OK (0) or a KTM_ERR_* code;
+ *     the void drop-ins record their status for ktmGetLastError().
+ */
+#ifndef KTM_H
+#define KTM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One image axis: axis[i] = imageStart + (float)i * imageStep.
+ * Field names from psktmFunctions.c:10-14 and psktmCUDA.cu:226-237; the
+ * reference defines no struct, so the field order is this library's. */
+struct imageGrid {
+    int   imagePnts;
+    float imageStep;
+    float imageStart;
+};
+
+/* Trace block description.  Field names from psktmCPU.c:29,59,82 and
+ * psktmCUDA.cu:245-247; traceSampleRate is the sample interval in seconds. */
+struct jobParams {
+    int   traceNo;
+    int   tracePts;
+    float traceSampleRate;
+};
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in entry points (host buffers, synchronous, image overwritten)      */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces ktmMigrationCPU, psktmCPU.c:13-23.  Same arguments, same result:
+ * the image is bit-identical to psktmCPU.c run with one thread (the reference
+ * loop races on image[] with more, psktmCPU.c:56-85).  Runs on the current
+ * CUDA device. */
+void ktmMigrationCPU(struct imageGrid* imageX, struct imageGrid* imageY,
+                     struct imageGrid* imageZ, struct jobParams* config,
+                     float* midX, float* midY, float* offX, float* offY,
+                     float* traces, float* slowness, float* image);
+
+/* Replaces ktmMigrationGPU, psktmCUDA.cu:211-221 (same signature as above).
+ * Unlike the reference GPU host it has no Nx*Ny block limit (:298-301), no
+ * traceNo % THREADS_X requirement (:95) and no Nz <= 2048 cap (:21-22). */
+void ktmMigrationGPU(struct imageGrid* imageX, struct imageGrid* imageY,
+                     struct imageGrid* imageZ, struct jobParams* config,
+                     float* midX, float* midY, float* offX, float* offY,
+                     float* traces, float* slowness, float* image);
+
+/* psktmFunctions.c:19-39 and :1-17 (host helpers, same arithmetic). */
+void initThreeAxes(struct imageGrid* imageX, struct imageGrid* imageY,
+                   struct imageGrid* imageZ, float* imageXX, float* imageYY,
+                   float* imageZZ);
+void initTwoAxes(struct imageGrid* imageY, struct imageGrid* imageZ,
+                 float* imageYY, float* imageZZ);
+
+/* ------------------------------------------------------------------------ */
+/* Status                                                                   */
+/* ------------------------------------------------------------------------ */
+
+enum {
+    KTM_OK = 0,
+    KTM_ERR_ARG = 1,        /* invalid argument (NULL pointer, bad size, bad enum) */
+    KTM_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    KTM_ERR_NOMEM = 3,      /* device or host allocation failed */
+    KTM_ERR_LIMIT = 4,      /* size beyond a documented kernel limit */
+    KTM_ERR_IO = 5,         /* file could not be opened / read / written */
+    KTM_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up */
+    KTM_ERR_NODEVICE = 7    /* no CUDA device visible */
+};
+
+/* Status of the most recent call made by this host thread. */
+int ktmGetLastError(void);
+/* Human-readable message for the most recent failure of this host thread. */
+const char* ktmGetLastErrorMessage(void);
+const char* ktmGetErrorString(int code);
+
+/* ------------------------------------------------------------------------ */
+/* Extended migration job                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Kernel family. */
+enum {
+    KTM_MODE_REFERENCE = 0, /* psktmCPU.c arithmetic, bit-exact: F32 traces,
+                               truncating pick, no aperture, 1-D velocity */
+    KTM_MODE_FAST = 1,      /* SFU square roots, linear or truncating pick,
+                               aperture, Vrms cube, F32/F16/BF16 traces */
+    KTM_MODE_F64 = 2        /* FP64 arithmetic (accuracy reference on device) */
+};
+
+/* Trace sample formats. */
+enum {
+    KTM_FMT_F32 = 0,
+    KTM_FMT_F16 = 1,        /* IEEE half, multiplied by a per-trace FP32 scale */
+    KTM_FMT_BF16 = 2        /* bfloat16, multiplied by a per-trace FP32 scale */
+};
+
+/* Sample pick. */
+enum {
+    KTM_PICK_TRUNCATE = 0,  /* it = (int)(t/dt), used when 0 < it < tracePts (psktmCPU.c:80-82) */
+    KTM_PICK_LINEAR = 1     /* linear interpolation between samples; samples
+                               outside 0 < j < tracePts read as zero */
+};
+
+typedef struct ktm_job {
+    struct imageGrid imageX, imageY, imageZ;   /* Z = one-way tau, s */
+    struct jobParams config;                   /* traceNo, tracePts, traceSampleRate */
+    const float* midX;                         /* [traceNo] */
+    const float* midY;
+    const float* offX;                         /* half offsets */
+    const float* offY;
+    const void*  traces;                       /* [traceNo][traceStride] in traceFormat */
+    const float* traceScale;                   /* [traceNo] for F16/BF16 (NULL: 1.0) */
+    int   traceFormat;                         /* KTM_FMT_* */
+    int   traceStride;                         /* samples between traces; 0 = tracePts */
+    int   tracesPrefolded;                     /* 1: samples already carry sqrt(j*dt)
+                                                  (ktmPrepareTraces weightPrefold=1) */
+    const float* velocity;                     /* m/s: [Nz], or [Nx][Ny][Nz] if velocityCube */
+    int   velocityCube;
+    float* image;                              /* [Nx][Ny][Nz] */
+    int   mode;                                /* KTM_MODE_* */
+    int   pick;                                /* KTM_PICK_* */
+    float aperture;                            /* max |mid - x| in metres; <= 0: off */
+    int   accumulate;                          /* 0: image overwritten, 1: added to */
+    int   deviceMemory;                        /* 1: every pointer is device memory;
+                                                  0: host memory, copied in and out */
+    void* stream;                              /* cudaStream_t (NULL: legacy default) */
+    int   tileRun;                             /* tau samples per thread (0: tuned) */
+    int   tileCols;                            /* image columns per CTA (0: tuned) */
+    unsigned long long* pairsEvaluated;        /* optional device counter: pairs the
+                                                  kernel evaluated (after culling) */
+} ktm_job;
+
+/* Zero-initialise a job and fill in defaults (mode FAST, pick LINEAR, F32,
+ * overwrite, host memory, tuned tiles). */
+void ktmJobInit(ktm_job* job);
+
+/* sizeof(ktm_job) as compiled into the library, for bindings (ctypes, cgo)
+ * that lay the struct out themselves.  No counterpart in the reference. */
+size_t ktmJobStructSize(void);
+
+/* Run one migration.  Asynchronous on job->stream when deviceMemory = 1;
+ * synchronous when host buffers are given.  Replaces the body of
+ * ktmMigrationCPU (psktmCPU.c:56-90) with the extended method. */
+int ktmMigrate(const ktm_job* job);
+
+/* FP64 device evaluation of the job's method (pick, aperture, Vrms cube,
+ * weight) for the image columns columns[0..ncols) (column index = ix*Ny + iy;
+ * columns == NULL: 0..ncols-1): out[q][Nz].  Device memory only.  Used to
+ * measure the error of the FP32 / FP16 / BF16 paths on images too large for a
+ * CPU evaluation.  No counterpart in the reference. */
+int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KTM_H */

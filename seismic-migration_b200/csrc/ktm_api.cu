@@ -1,0 +1,292 @@
+// ktm_api.cu -- the C ABI of libktm.so: status, the drop-in entry points that
+// replace ktmMigrationCPU / ktmMigrationGPU, and the extended job API.
+#include "ktm_internal.cuh"
+
+#include <cstdarg>
+#include <cstring>
+#include <vector>
+
+namespace ktm {
+
+namespace {
+thread_local int tl_code = KTM_OK;
+thread_local char tl_msg[512] = "";
+}  // namespace
+
+int set_error(int code, const char* fmt, ...)
+{
+    tl_code = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(tl_msg, sizeof(tl_msg), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int set_ok()
+{
+    tl_code = KTM_OK;
+    tl_msg[0] = 0;
+    return KTM_OK;
+}
+
+namespace {
+
+bool grid_ok(const imageGrid& g) { return g.imagePnts >= 0; }
+
+int make_geometry(const ktm_job* j, Geometry* g)
+{
+    if (!grid_ok(j->imageX) || !grid_ok(j->imageY) || !grid_ok(j->imageZ))
+        return set_error(KTM_ERR_ARG, "image axis with negative point count");
+    if (j->config.traceNo < 0 || j->config.tracePts < 0)
+        return set_error(KTM_ERR_ARG, "negative traceNo or tracePts");
+    if (!(j->config.traceSampleRate > 0.0f))
+        return set_error(KTM_ERR_ARG, "traceSampleRate must be > 0");
+    const long long cols = (long long)j->imageX.imagePnts * j->imageY.imagePnts;
+    if (cols > 0x7fffffffLL || cols * j->imageZ.imagePnts > (1LL << 40))
+        return set_error(KTM_ERR_LIMIT, "image too large");
+    g->nx = j->imageX.imagePnts; g->ny = j->imageY.imagePnts; g->nz = j->imageZ.imagePnts;
+    g->x0 = j->imageX.imageStart; g->dx = j->imageX.imageStep;
+    g->y0 = j->imageY.imageStart; g->dy = j->imageY.imageStep;
+    g->z0 = j->imageZ.imageStart; g->dz = j->imageZ.imageStep;
+    g->ntr = j->config.traceNo; g->nt = j->config.tracePts;
+    g->stride = j->traceStride > 0 ? j->traceStride : j->config.tracePts;
+    if (g->stride < g->nt) return set_error(KTM_ERR_ARG, "traceStride < tracePts");
+    g->dt = j->config.traceSampleRate;
+    return KTM_OK;
+}
+
+size_t fmt_bytes(int fmt) { return fmt == KTM_FMT_F32 ? 4 : 2; }
+
+// Device copies of a host-memory job (freed in the destructor, stream-ordered).
+struct Staged {
+    cudaStream_t s;
+    std::vector<void*> ptrs;
+    explicit Staged(cudaStream_t st) : s(st) {}
+    ~Staged()
+    {
+        for (void* p : ptrs) cudaFreeAsync(p, s);
+    }
+    int alloc(void** p, size_t bytes)
+    {
+        *p = nullptr;
+        if (bytes == 0) return KTM_OK;
+        KTM_CUDA_TRY(cudaMallocAsync(p, bytes, s));
+        ptrs.push_back(*p);
+        return KTM_OK;
+    }
+    template <class T>
+    int upload(const T* host, size_t bytes, const T** dev)
+    {
+        *dev = nullptr;
+        if (!host || bytes == 0) return KTM_OK;
+        void* d;
+        int rc = alloc(&d, bytes);
+        if (rc) return rc;
+        KTM_CUDA_TRY(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, s));
+        *dev = static_cast<const T*>(d);
+        return KTM_OK;
+    }
+};
+
+int run_device(const ktm_job* j, const Geometry& g, const float* midX, const float* midY,
+               const float* offX, const float* offY, const void* traces, const float* scale,
+               const float* vel, float* image, cudaStream_t s)
+{
+    if (j->mode == KTM_MODE_REFERENCE) {
+        if (j->traceFormat != KTM_FMT_F32 || j->pick != KTM_PICK_TRUNCATE || j->velocityCube ||
+            j->aperture > 0.0f || j->tracesPrefolded || scale)
+            return set_error(KTM_ERR_ARG,
+                             "reference mode takes F32 traces, truncating pick, no aperture, "
+                             "no scale and a 1-D velocity (psktmCPU.c semantics)");
+        return launch_reference(g, midX, midY, offX, offY, static_cast<const float*>(traces), vel,
+                                image, j->accumulate, j->tileRun, s);
+    }
+    if (j->mode == KTM_MODE_FAST) {
+        FastArgs a;
+        a.g = g; a.midX = midX; a.midY = midY; a.offX = offX; a.offY = offY;
+        a.traces = traces; a.scale = scale; a.fmt = j->traceFormat;
+        a.weightMode = j->tracesPrefolded ? 2 : (j->pick == KTM_PICK_LINEAR ? 1 : 0);
+        a.vel = vel; a.velCube = j->velocityCube;
+        a.image = image; a.accumulate = j->accumulate;
+        a.pick = j->pick; a.aperture = j->aperture;
+        a.tileRun = j->tileRun; a.tileCols = j->tileCols;
+        a.pairsEvaluated = j->pairsEvaluated;
+        return launch_fast(a, s);
+    }
+    return set_error(KTM_ERR_ARG, "ktmMigrate: mode must be REFERENCE or FAST "
+                                  "(FP64 output goes through ktmMigrateColumnsF64)");
+}
+
+int check_job(const ktm_job* j)
+{
+    if (!j) return set_error(KTM_ERR_ARG, "NULL job");
+    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_BF16)
+        return set_error(KTM_ERR_ARG, "bad traceFormat %d", j->traceFormat);
+    if (j->pick != KTM_PICK_TRUNCATE && j->pick != KTM_PICK_LINEAR)
+        return set_error(KTM_ERR_ARG, "bad pick %d", j->pick);
+    const bool needTraces = j->config.traceNo > 0;
+    if (needTraces && (!j->midX || !j->midY || !j->offX || !j->offY || !j->traces))
+        return set_error(KTM_ERR_ARG, "NULL coordinate or trace pointer");
+    if (!j->velocity && (long long)j->imageZ.imagePnts > 0)
+        return set_error(KTM_ERR_ARG, "NULL velocity");
+    if (!j->image && (long long)j->imageX.imagePnts * j->imageY.imagePnts * j->imageZ.imagePnts > 0)
+        return set_error(KTM_ERR_ARG, "NULL image");
+    return KTM_OK;
+}
+
+int migrate_impl(const ktm_job* j)
+{
+    int rc = check_job(j);
+    if (rc) return rc;
+    Geometry g;
+    rc = make_geometry(j, &g);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(j->stream);
+    if (j->deviceMemory) {
+        rc = run_device(j, g, j->midX, j->midY, j->offX, j->offY, j->traces, j->traceScale,
+                        j->velocity, j->image, s);
+        return rc ? rc : set_ok();
+    }
+    // host buffers: copy in, run, copy out, synchronise
+    const size_t ntr = (size_t)g.ntr, nimg = (size_t)g.nx * g.ny * g.nz;
+    const size_t nvel = j->velocityCube ? nimg : (size_t)g.nz;
+    const float *dmx, *dmy, *dox, *doy, *dsc, *dvel;
+    const unsigned char* dtr;
+    void* dimg = nullptr;
+    {
+        Staged st(s);
+        if ((rc = st.upload(j->midX, ntr * 4, &dmx)) || (rc = st.upload(j->midY, ntr * 4, &dmy)) ||
+            (rc = st.upload(j->offX, ntr * 4, &dox)) || (rc = st.upload(j->offY, ntr * 4, &doy)) ||
+            (rc = st.upload(static_cast<const unsigned char*>(j->traces),
+                            ntr * g.stride * fmt_bytes(j->traceFormat), &dtr)) ||
+            (rc = st.upload(j->traceScale, j->traceScale ? ntr * 4 : 0, &dsc)) ||
+            (rc = st.upload(j->velocity, nvel * 4, &dvel)) || (rc = st.alloc(&dimg, nimg * 4)))
+            return rc;
+        if (j->accumulate && nimg)
+            KTM_CUDA_TRY(cudaMemcpyAsync(dimg, j->image, nimg * 4, cudaMemcpyHostToDevice, s));
+        rc = run_device(j, g, dmx, dmy, dox, doy, dtr, dsc, dvel, static_cast<float*>(dimg), s);
+        if (rc) return rc;
+        if (nimg)
+            KTM_CUDA_TRY(cudaMemcpyAsync(j->image, dimg, nimg * 4, cudaMemcpyDeviceToHost, s));
+    }
+    KTM_CUDA_TRY(cudaStreamSynchronize(s));
+    return set_ok();
+}
+
+void dropin(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* config,
+            float* midX, float* midY, float* offX, float* offY, float* traces, float* slowness,
+            float* image)
+{
+    if (!imageX || !imageY || !imageZ || !config) {
+        set_error(KTM_ERR_ARG, "NULL grid or config");
+        return;
+    }
+    ktm_job j;
+    ktmJobInit(&j);
+    j.imageX = *imageX; j.imageY = *imageY; j.imageZ = *imageZ; j.config = *config;
+    j.midX = midX; j.midY = midY; j.offX = offX; j.offY = offY;
+    j.traces = traces; j.velocity = slowness; j.image = image;
+    j.mode = KTM_MODE_REFERENCE;
+    j.pick = KTM_PICK_TRUNCATE;
+    j.deviceMemory = 0;
+    migrate_impl(&j);
+}
+
+}  // namespace
+}  // namespace ktm
+
+extern "C" {
+
+int ktmGetLastError(void) { return ktm::tl_code; }
+const char* ktmGetLastErrorMessage(void) { return ktm::tl_msg; }
+
+const char* ktmGetErrorString(int code)
+{
+    switch (code) {
+        case KTM_OK: return "ok";
+        case KTM_ERR_ARG: return "invalid argument";
+        case KTM_ERR_CUDA: return "CUDA runtime error";
+        case KTM_ERR_NOMEM: return "out of memory";
+        case KTM_ERR_LIMIT: return "size beyond a kernel limit";
+        case KTM_ERR_IO: return "file I/O error";
+        case KTM_ERR_TIMEOUT: return "device wait timed out";
+        case KTM_ERR_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+void ktmJobInit(ktm_job* job)
+{
+    if (!job) return;
+    std::memset(job, 0, sizeof(*job));
+    job->mode = KTM_MODE_FAST;
+    job->pick = KTM_PICK_LINEAR;
+    job->traceFormat = KTM_FMT_F32;
+}
+
+int ktmMigrate(const ktm_job* job) { return ktm::migrate_impl(job); }
+
+size_t ktmJobStructSize(void) { return sizeof(ktm_job); }
+
+void ktmMigrationCPU(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* config,
+                     float* midX, float* midY, float* offX, float* offY, float* traces,
+                     float* slowness, float* image)
+{
+    ktm::dropin(imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness, image);
+}
+
+void ktmMigrationGPU(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* config,
+                     float* midX, float* midY, float* offX, float* offY, float* traces,
+                     float* slowness, float* image)
+{
+    ktm::dropin(imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness, image);
+}
+
+void initThreeAxes(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, float* imageXX,
+                   float* imageYY, float* imageZZ)
+{
+    // psktmFunctions.c:26-33 (host code built with -ffp-contract=off: the product
+    // and the sum are rounded separately, as in the reference build)
+    for (int i = 0; i < imageX->imagePnts; i++) {
+        float p = (float)i * imageX->imageStep;
+        imageXX[i] = imageX->imageStart + p;
+    }
+    initTwoAxes(imageY, imageZ, imageYY, imageZZ);
+}
+
+void initTwoAxes(imageGrid* imageY, imageGrid* imageZ, float* imageYY, float* imageZZ)
+{
+    // psktmFunctions.c:9-13
+    for (int i = 0; i < imageY->imagePnts; i++) {
+        float p = (float)i * imageY->imageStep;
+        imageYY[i] = imageY->imageStart + p;
+    }
+    for (int i = 0; i < imageZ->imagePnts; i++) {
+        float p = (float)i * imageZ->imageStep;
+        imageZZ[i] = imageZ->imageStart + p;
+    }
+}
+
+int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, double* out)
+{
+    int rc = ktm::check_job(job);
+    if (rc) return rc;
+    if (!job->deviceMemory)
+        return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64 takes device memory");
+    if (ncols < 0 || (!out && ncols > 0)) return ktm::set_error(KTM_ERR_ARG, "bad column list");
+    ktm::Geometry g;
+    rc = ktm::make_geometry(job, &g);
+    if (rc) return rc;
+    ktm::FastArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = g; a.midX = job->midX; a.midY = job->midY; a.offX = job->offX; a.offY = job->offY;
+    a.traces = job->traces; a.scale = job->traceScale; a.fmt = job->traceFormat;
+    a.weightMode = job->tracesPrefolded ? 2 : 0;
+    a.vel = job->velocity; a.velCube = job->velocityCube;
+    a.pick = job->pick; a.aperture = job->aperture;
+    rc = ktm::launch_f64_columns(a, columns, ncols, out, static_cast<cudaStream_t>(job->stream));
+    return rc ? rc : ktm::set_ok();
+}
+
+}  // extern "C"

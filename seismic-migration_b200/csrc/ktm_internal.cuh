@@ -1,0 +1,67 @@
+// ktm_internal.cuh -- shared declarations of libktm.so (not installed; the
+// public ABI is include/ktm.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/ktm.h"
+
+namespace ktm {
+
+// ---------------------------------------------------------------- status ---
+// Records the status of the calling host thread (ktmGetLastError).
+int set_error(int code, const char* fmt, ...);
+int set_ok();
+
+#define KTM_CUDA_TRY(expr)                                                      \
+    do {                                                                        \
+        cudaError_t e_ = (expr);                                                \
+        if (e_ != cudaSuccess)                                                  \
+            return ::ktm::set_error(e_ == cudaErrorMemoryAllocation             \
+                                        ? KTM_ERR_NOMEM : KTM_ERR_CUDA,         \
+                                    "%s: %s (%s:%d)", #expr,                    \
+                                    cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+// ----------------------------------------------------------- kernel args ---
+// Image axes and the trace block, as the kernels see them.
+struct Geometry {
+    int nx, ny, nz;
+    float x0, dx, y0, dy, z0, dz;  // axis[i] = start + (float)i * step
+    int ntr, nt, stride;           // traces, samples per trace, samples between traces
+    float dt;                      // trace sample interval, s
+};
+
+// Largest dynamic shared memory a kernel here asks for (B200: 227 KB per CTA).
+constexpr int kMaxSmemBytes = 227 * 1024;
+
+// Reference-mode kernel launch (ktm_ref.cu).  All pointers are device memory.
+int launch_reference(const Geometry& g, const float* midX, const float* midY,
+                     const float* offX, const float* offY, const float* traces,
+                     const float* vel, float* image, int accumulate, int tileRun,
+                     cudaStream_t stream);
+
+// Fast kernel launch (ktm_fast.cu).  All pointers are device memory.
+struct FastArgs {
+    Geometry g;
+    const float* midX; const float* midY; const float* offX; const float* offY;
+    const void* traces; const float* scale; int fmt;
+    // 0: weight sqrt(t) per pair; 1: sqrt(j*dt) multiplied into each staged
+    // sample; 2: stored samples already carry sqrt(j*dt)
+    int weightMode;
+    const float* vel; int velCube;
+    float* image; int accumulate;
+    int pick; float aperture;
+    int tileRun, tileCols;
+    unsigned long long* pairsEvaluated;
+};
+int launch_fast(const FastArgs& a, cudaStream_t stream);
+
+// FP64 device reference (ktm_fast.cu): out[q][nz] for image columns cols[q]
+// (cols == NULL: columns 0..ncols-1).
+int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* out,
+                       cudaStream_t stream);
+
+}  // namespace ktm

@@ -1,0 +1,11 @@
+"""ktm -- B200 prestack Kirchhoff time migration (PSTM), Python host side.
+
+The compute lives in ``libktm.so`` (hand-written sm_100a CUDA behind the C ABI
+of include/ktm.h); this package binds it with ctypes, mirrors the reference's
+entry points (``ktmMigrationCPU`` and friends) and generates the seeded
+synthetic surveys used by the tests and the benchmark.
+"""
+from ._lib import KtmError, ImageGrid, JobParams, lib, LIB_PATH  # noqa: F401
+from .api import (  # noqa: F401
+    grid, ktmMigrationCPU, ktmMigrationGPU, initThreeAxes, migrate, migrate_columns_f64, Job,
+)

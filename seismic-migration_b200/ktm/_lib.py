@@ -1,0 +1,134 @@
+"""ctypes binding of libktm.so (the C ABI declared in include/ktm.h).
+
+The library is built in-tree by ``seismic-migration_b200/build.py``.  There is
+no fallback: if ``libktm.so`` is missing or cannot be loaded, every call fails
+with ``KtmError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libktm.so")
+
+# status codes (ktm.h)
+KTM_OK = 0
+KTM_ERR_ARG = 1
+KTM_ERR_CUDA = 2
+KTM_ERR_NOMEM = 3
+KTM_ERR_LIMIT = 4
+KTM_ERR_IO = 5
+KTM_ERR_TIMEOUT = 6
+KTM_ERR_NODEVICE = 7
+
+KTM_MODE_REFERENCE, KTM_MODE_FAST, KTM_MODE_F64 = 0, 1, 2
+KTM_FMT_F32, KTM_FMT_F16, KTM_FMT_BF16 = 0, 1, 2
+KTM_PICK_TRUNCATE, KTM_PICK_LINEAR = 0, 1
+KTM_RHO_NONE, KTM_RHO_2D, KTM_RHO_25D, KTM_RHO_3D = 0, 1, 2, 3
+
+
+class KtmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ktm error {code}: {msg}")
+        self.code = code
+
+
+class ImageGrid(C.Structure):
+    """struct imageGrid (psktmFunctions.c:10-14 field names)."""
+    _fields_ = [("imagePnts", C.c_int), ("imageStep", C.c_float), ("imageStart", C.c_float)]
+
+    def axis(self):
+        import numpy as np
+        i = np.arange(self.imagePnts, dtype=np.float32)
+        return (np.float32(self.imageStart) + i * np.float32(self.imageStep)).astype(np.float32)
+
+
+class JobParams(C.Structure):
+    """struct jobParams (psktmCPU.c:29,59,82 field names)."""
+    _fields_ = [("traceNo", C.c_int), ("tracePts", C.c_int), ("traceSampleRate", C.c_float)]
+
+
+P = C.c_void_p
+
+
+class KtmJob(C.Structure):
+    """ktm_job (include/ktm.h)."""
+    _fields_ = [
+        ("imageX", ImageGrid), ("imageY", ImageGrid), ("imageZ", ImageGrid),
+        ("config", JobParams),
+        ("midX", P), ("midY", P), ("offX", P), ("offY", P),
+        ("traces", P), ("traceScale", P),
+        ("traceFormat", C.c_int), ("traceStride", C.c_int), ("tracesPrefolded", C.c_int),
+        ("velocity", P), ("velocityCube", C.c_int),
+        ("image", P),
+        ("mode", C.c_int), ("pick", C.c_int), ("aperture", C.c_float),
+        ("accumulate", C.c_int), ("deviceMemory", C.c_int),
+        ("stream", P),
+        ("tileRun", C.c_int), ("tileCols", C.c_int),
+        ("pairsEvaluated", P),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libktm.so once; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise KtmError(-1, f"{LIB_PATH} is not built: run seismic-migration_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    G = C.POINTER(ImageGrid)
+    J = C.POINTER(JobParams)
+    L.ktmMigrationCPU.argtypes = [G, G, G, J] + [P] * 7
+    L.ktmMigrationCPU.restype = None
+    L.ktmMigrationGPU.argtypes = [G, G, G, J] + [P] * 7
+    L.ktmMigrationGPU.restype = None
+    L.initThreeAxes.argtypes = [G, G, G, P, P, P]
+    L.initThreeAxes.restype = None
+    L.initTwoAxes.argtypes = [G, G, P, P]
+    L.initTwoAxes.restype = None
+    L.ktmGetLastError.restype = C.c_int
+    L.ktmGetLastErrorMessage.restype = C.c_char_p
+    L.ktmGetErrorString.argtypes = [C.c_int]
+    L.ktmGetErrorString.restype = C.c_char_p
+    L.ktmJobInit.argtypes = [C.POINTER(KtmJob)]
+    L.ktmJobInit.restype = None
+    L.ktmJobStructSize.restype = C.c_size_t
+    L.ktmMigrate.argtypes = [C.POINTER(KtmJob)]
+    L.ktmMigrate.restype = C.c_int
+    L.ktmMigrateColumnsF64.argtypes = [C.POINTER(KtmJob), P, C.c_int, P]
+    L.ktmMigrateColumnsF64.restype = C.c_int
+    _optional(L)
+    if L.ktmJobStructSize() != C.sizeof(KtmJob):
+        raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "
+                           f"binding {C.sizeof(KtmJob)} bytes")
+    _lib = L
+    return L
+
+
+def _optional(L) -> None:
+    """Signatures of the entry points added alongside the migration."""
+    for name, args, res in _EXTRA:
+        fn = getattr(L, name, None)
+        if fn is not None:
+            fn.argtypes = args
+            fn.restype = res
+
+
+_EXTRA: list = []
+
+
+def check(rc: int) -> None:
+    if rc != KTM_OK:
+        L = lib()
+        raise KtmError(rc, L.ktmGetLastErrorMessage().decode(errors="replace")
+                       or L.ktmGetErrorString(rc).decode())
+
+
+def last_error() -> tuple[int, str]:
+    L = lib()
+    return L.ktmGetLastError(), L.ktmGetLastErrorMessage().decode(errors="replace")

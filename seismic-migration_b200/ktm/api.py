@@ -1,0 +1,183 @@
+"""Python mirror of the reference's PSTM interface over libktm.so.
+
+``ktmMigrationCPU`` / ``ktmMigrationGPU`` keep the argument list of
+psktmCPU.c:13-23 (grids, config, mid/off vectors, traces, velocity, image);
+``migrate`` is the extended job (``ktmMigrate`` in include/ktm.h).  Arrays are
+numpy (host memory: the library copies in and out) or CUDA torch tensors
+(device memory: the call is asynchronous on the given stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import ImageGrid, JobParams, KtmError, KtmJob, check, lib
+
+_PICK = {"truncate": _lib.KTM_PICK_TRUNCATE, "linear": _lib.KTM_PICK_LINEAR}
+_MODE = {"reference": _lib.KTM_MODE_REFERENCE, "fast": _lib.KTM_MODE_FAST}
+_FMT = {"f32": _lib.KTM_FMT_F32, "f16": _lib.KTM_FMT_F16, "bf16": _lib.KTM_FMT_BF16}
+
+
+def grid(n: int, step: float, start: float = 0.0) -> ImageGrid:
+    return ImageGrid(int(n), float(step), float(start))
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _dropin(fn, imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness,
+            image=None) -> np.ndarray:
+    midX, midY, offX, offY, traces, slowness = map(_f32, (midX, midY, offX, offY, traces,
+                                                          slowness))
+    shape = (imageX.imagePnts, imageY.imagePnts, imageZ.imagePnts)
+    if image is None:
+        image = np.empty(shape, np.float32)
+    if image.dtype != np.float32 or not image.flags.c_contiguous or image.size != np.prod(shape):
+        raise ValueError("image must be a contiguous float32 array of Nx*Ny*Nz values")
+    if traces.size < config.traceNo * config.tracePts:
+        raise ValueError("traces holds fewer than traceNo*tracePts samples")
+    L = lib()
+    getattr(L, fn)(C.byref(imageX), C.byref(imageY), C.byref(imageZ), C.byref(config),
+                   midX.ctypes.data, midY.ctypes.data, offX.ctypes.data, offY.ctypes.data,
+                   traces.ctypes.data, slowness.ctypes.data, image.ctypes.data)
+    code, msg = _lib.last_error()
+    if code:
+        raise KtmError(code, msg)
+    return image
+
+
+def ktmMigrationCPU(imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness,
+                    image=None) -> np.ndarray:
+    """psktmCPU.c:13-23 on the GPU: bit-identical image, overwritten."""
+    return _dropin("ktmMigrationCPU", imageX, imageY, imageZ, config, midX, midY, offX, offY,
+                   traces, slowness, image)
+
+
+def ktmMigrationGPU(imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness,
+                    image=None) -> np.ndarray:
+    """psktmCUDA.cu:211-221 signature; same result as ktmMigrationCPU."""
+    return _dropin("ktmMigrationGPU", imageX, imageY, imageZ, config, midX, midY, offX, offY,
+                   traces, slowness, image)
+
+
+def initThreeAxes(imageX, imageY, imageZ):
+    xx = np.empty(imageX.imagePnts, np.float32)
+    yy = np.empty(imageY.imagePnts, np.float32)
+    zz = np.empty(imageZ.imagePnts, np.float32)
+    lib().initThreeAxes(C.byref(imageX), C.byref(imageY), C.byref(imageZ), xx.ctypes.data,
+                        yy.ctypes.data, zz.ctypes.data)
+    return xx, yy, zz
+
+
+# ------------------------------------------------------------------------------------------
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_torch(a):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class Job:
+    """Builds a ktm_job and keeps every array it points at alive."""
+
+    def __init__(self, *, imageX, imageY, imageZ, dt, midX, midY, offX, offY, traces,
+                 velocity, image=None, scale=None, mode="fast", pick="linear",
+                 aperture=0.0, accumulate=False, prefolded=False, fmt=None, stream=None,
+                 tile_run=0, pairs_counter=None, trace_stride=0):
+        dev = _is_torch(traces)
+        self.device = dev
+        self.keep = []
+        nx, ny, nz = imageX.imagePnts, imageY.imagePnts, imageZ.imagePnts
+        if dev:
+            import torch
+            if not traces.is_cuda:
+                raise ValueError("torch tensors must be CUDA tensors")
+            ntr = traces.shape[0]
+            nt = traces.shape[1] if trace_stride == 0 else trace_stride
+            if fmt is None:
+                fmt = {torch.float32: "f32", torch.float16: "f16", torch.bfloat16: "bf16"}[traces.dtype]
+            if image is None:
+                image = torch.empty((nx, ny, nz), device=traces.device, dtype=torch.float32)
+            for a in (midX, midY, offX, offY, velocity, image, scale):
+                if a is not None and not a.is_contiguous():
+                    raise ValueError("device arrays must be contiguous")
+        else:
+            traces = np.ascontiguousarray(traces)
+            if fmt is None:
+                fmt = {np.dtype(np.float32): "f32", np.dtype(np.float16): "f16"}.get(
+                    traces.dtype, "f32")
+                if fmt == "f32":
+                    traces = _f32(traces)
+            midX, midY, offX, offY, velocity = map(_f32, (midX, midY, offX, offY, velocity))
+            if scale is not None:
+                scale = _f32(scale)
+            if image is None:
+                image = np.zeros((nx, ny, nz), np.float32)
+            ntr = traces.shape[0]
+            nt = traces.shape[1] if trace_stride == 0 else trace_stride
+        self.image = image
+        self.keep += [midX, midY, offX, offY, traces, velocity, image, scale]
+        j = KtmJob()
+        lib().ktmJobInit(C.byref(j))
+        j.imageX, j.imageY, j.imageZ = imageX, imageY, imageZ
+        j.config = JobParams(int(ntr), int(nt), float(dt))
+        j.midX, j.midY, j.offX, j.offY = map(_ptr, (midX, midY, offX, offY))
+        j.traces = _ptr(traces)
+        j.traceScale = _ptr(scale)
+        j.traceFormat = _FMT[fmt]
+        j.traceStride = int(trace_stride)
+        j.tracesPrefolded = int(bool(prefolded))
+        j.velocity = _ptr(velocity)
+        j.velocityCube = int(len(velocity.shape) == 3)
+        j.image = _ptr(image)
+        j.mode = _MODE[mode]
+        j.pick = _PICK[pick]
+        j.aperture = float(aperture)
+        j.accumulate = int(bool(accumulate))
+        j.deviceMemory = int(dev)
+        j.stream = _stream_handle(stream)
+        j.tileRun = int(tile_run)
+        j.pairsEvaluated = _ptr(pairs_counter)
+        self.job = j
+
+    def run(self):
+        check(lib().ktmMigrate(C.byref(self.job)))
+        return self.image
+
+
+def migrate(**kw):
+    """One migration (ktmMigrate).  Returns the image array / tensor."""
+    return Job(**kw).run()
+
+
+def migrate_columns_f64(*, columns=None, ncols=None, **kw):
+    """FP64 device evaluation for a list of image columns -> torch float64 [ncols, Nz]."""
+    import torch
+    job = Job(**kw)
+    if not job.device:
+        raise ValueError("migrate_columns_f64 takes CUDA tensors")
+    nz = kw["imageZ"].imagePnts
+    if columns is not None:
+        cols = columns.to(device=kw["traces"].device, dtype=torch.int32).contiguous()
+        n = cols.numel()
+    else:
+        cols, n = None, int(ncols)
+    out = torch.empty((n, nz), device=kw["traces"].device, dtype=torch.float64)
+    check(lib().ktmMigrateColumnsF64(C.byref(job.job), _ptr(cols), int(n), out.data_ptr()))
+    return out

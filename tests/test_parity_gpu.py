@@ -1,0 +1,201 @@
+"""Parity of the CUDA kernels with the reference and the oracle (needs a B200).
+
+* reference mode / the drop-in entry points: bit-identical to the reference's
+  own psktmCPU.c (golden fixtures) and to the oracle restatement on random cases;
+* fast mode: within stated tolerances of the FP64 oracle, FP32 / FP16 / BF16
+  trace storage, aperture, laterally varying velocity, both picks;
+* edge cases: empty trace sets, ragged sizes (trace counts not multiples of
+  the chunk, Nz not a multiple of the run, Nx*Ny not a multiple of the CTA's
+  columns), accumulation, host vs device memory.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN_MIGRATIONS, golden_grids, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def random_case(seed, ntr=53, nt=140, nx=5, ny=3, nz=101, dt=0.004, dz=0.002, spread=300.0):
+    rng = np.random.default_rng(seed)
+    gx, gy, gz = oracle.grid(nx, 30.0, -60.0), oracle.grid(ny, 25.0, -20.0), oracle.grid(nz, dz, 0.0)
+    mid = rng.uniform(-spread, spread, (ntr, 2)).astype(np.float32)
+    off = rng.uniform(-spread, spread, (ntr, 2)).astype(np.float32)
+    tr = rng.standard_normal((ntr, nt)).astype(np.float32)
+    vel = np.linspace(1500.0, 3000.0, nz).astype(np.float32)
+    return gx, gy, gz, dt, mid[:, 0].copy(), mid[:, 1].copy(), off[:, 0].copy(), off[:, 1].copy(), tr, vel
+
+
+# ------------------------------------------------------------------ reference mode ----
+@pytest.mark.parametrize("name", GOLDEN_MIGRATIONS)
+@pytest.mark.parametrize("entry", ["ktmMigrationCPU", "ktmMigrationGPU"])
+def test_dropin_bit_identical_to_reference_golden(cuda, ktm_lib, name, entry):
+    import ktm
+    g = load_golden(name)
+    gx, gy, gz = golden_grids(g)
+    cfg = ktm.JobParams(g["traces"].shape[0], g["traces"].shape[1], float(g["dt"]))
+    img = getattr(ktm, entry)(gx, gy, gz, cfg, g["midX"], g["midY"], g["offX"], g["offY"],
+                              g["traces"], g["velocity"])
+    assert np.array_equal(img.view(np.uint32), g["image"].view(np.uint32))
+
+
+@pytest.mark.parametrize("seed,ntr,nx,ny,nz", [(0, 53, 5, 3, 101), (1, 300, 9, 1, 1001),
+                                                (2, 1, 1, 1, 7), (3, 77, 13, 2, 515)])
+def test_reference_mode_bit_identical_to_oracle_random(cuda, ktm_lib, seed, ntr, nx, ny, nz):
+    import ktm
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = random_case(seed, ntr=ntr, nx=nx, ny=ny, nz=nz)
+    ref = oracle.migrate_ref32(gx, gy, gz, dt, mx, my, ox, oy, tr, vel)
+    cfg = ktm.JobParams(ntr, tr.shape[1], dt)
+    img = ktm.ktmMigrationCPU(gx, gy, gz, cfg, mx, my, ox, oy, tr, vel)
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+
+
+def test_reference_mode_device_memory_and_accumulate(cuda, ktm_lib):
+    import ktm
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = random_case(4, ntr=40, nz=64)
+    ref = oracle.migrate_ref32(gx, gy, gz, dt, mx, my, ox, oy, tr, vel)
+    kw = dict(imageX=gx, imageY=gy, imageZ=gz, dt=dt, mode="reference", pick="truncate")
+    img = ktm.migrate(midX=_t(mx, cuda), midY=_t(my, cuda), offX=_t(ox, cuda), offY=_t(oy, cuda),
+                      traces=_t(tr, cuda), velocity=_t(vel, cuda), **kw)
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    # accumulate = 1 adds onto the image already there
+    img2 = ktm.migrate(midX=_t(mx, cuda), midY=_t(my, cuda), offX=_t(ox, cuda), offY=_t(oy, cuda),
+                       traces=_t(tr, cuda), velocity=_t(vel, cuda), image=img.clone(),
+                       accumulate=True, **kw)
+    assert np.array_equal(img2.cpu().numpy(), (ref + ref).astype(np.float32))
+
+
+def test_empty_trace_set_gives_zero_image(cuda, ktm_lib):
+    import ktm
+    gx, gy, gz = ktm.grid(4, 10.0), ktm.grid(2, 10.0), ktm.grid(30, 0.002)
+    e = np.zeros(0, np.float32)
+    img = ktm.ktmMigrationCPU(gx, gy, gz, ktm.JobParams(0, 50, 0.004), e, e, e, e,
+                              np.zeros((0, 50), np.float32), np.full(30, 2000.0, np.float32),
+                              image=np.full((4, 2, 30), 7.0, np.float32))
+    assert not img.any()
+    for mode, pick in (("fast", "linear"), ("reference", "truncate")):
+        img = ktm.migrate(imageX=gx, imageY=gy, imageZ=gz, dt=0.004, midX=e, midY=e, offX=e,
+                          offY=e, traces=np.zeros((0, 50), np.float32),
+                          velocity=np.full(30, 2000.0, np.float32), mode=mode, pick=pick)
+        assert not img.any()
+
+
+# ----------------------------------------------------------------------- fast mode ----
+def fast(dev, case, **kw):
+    import ktm
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    return ktm.migrate(imageX=gx, imageY=gy, imageZ=gz, dt=dt, midX=_t(mx, dev), midY=_t(my, dev),
+                       offX=_t(ox, dev), offY=_t(oy, dev), traces=_t(tr, dev),
+                       velocity=_t(vel, dev), **kw).cpu().numpy()
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_fast_linear_matches_f64_oracle(cuda, ktm_lib, seed):
+    case = random_case(seed, ntr=120, nz=257)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    img = fast(cuda, case, pick="linear")
+    # same formulation (sqrt(j dt) per sample, then interpolation): FP32 rounding only
+    ref1 = oracle.migrate_f64(*case, pick=1, prefold=1)
+    assert rel_l2(img, ref1) < 2e-5
+    # against the reference weight |tau| sqrt(t) per pair: the accuracy gate
+    ref0 = oracle.migrate_f64(*case, pick=1, prefold=0)
+    assert rel_l2(img, ref0) < 1e-3
+
+
+def test_fast_truncate_matches_f64_oracle(cuda, ktm_lib):
+    case = random_case(7, ntr=90, nz=200)
+    img = fast(cuda, case, pick="truncate")
+    ref = oracle.migrate_f64(*case, pick=0, prefold=0)
+    # a truncated index flips where t/dt is within FP32 rounding of an integer
+    assert rel_l2(img, ref) < 2e-3
+
+
+def test_fast_aperture_and_velocity_cube(cuda, ktm_lib):
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = random_case(3, ntr=150, nx=6, ny=4, nz=180)
+    rng = np.random.default_rng(3)
+    cube = (vel[None, None, :] * rng.uniform(0.9, 1.1, (6, 4, 1))).astype(np.float32)
+    case = (gx, gy, gz, dt, mx, my, ox, oy, tr, cube)
+    img = fast(cuda, case, pick="linear", aperture=220.0)
+    ref = oracle.migrate_f64(*case, pick=1, prefold=1, aperture=220.0)
+    assert rel_l2(img, ref) < 2e-5
+    full = oracle.migrate_f64(*case, pick=1, prefold=1)
+    assert rel_l2(ref, full) > 1e-2      # the aperture removed something
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+def test_fast_half_storage_with_scale(cuda, ktm_lib, fmt):
+    import torch
+    import ktm
+    case = random_case(11, ntr=200, nz=300)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    tr = tr * np.random.default_rng(1).uniform(0.01, 100.0, (tr.shape[0], 1)).astype(np.float32)
+    scale = (np.abs(tr).max(axis=1) / 1.0).astype(np.float32)
+    q = torch.as_tensor(tr / scale[:, None]).to(cuda).to(torch.float16 if fmt == "f16" else torch.bfloat16)
+    img = ktm.migrate(imageX=gx, imageY=gy, imageZ=gz, dt=dt, midX=_t(mx, cuda), midY=_t(my, cuda),
+                      offX=_t(ox, cuda), offY=_t(oy, cuda), traces=q, scale=_t(scale, cuda),
+                      velocity=_t(vel, cuda), pick="linear").cpu().numpy()
+    qf = q.float().cpu().numpy()
+    same = oracle.migrate_f64(gx, gy, gz, dt, mx, my, ox, oy, qf, vel, scale=scale, pick=1, prefold=1)
+    assert rel_l2(img, same) < 2e-5
+    ref0 = oracle.migrate_f64(gx, gy, gz, dt, mx, my, ox, oy, tr, vel, pick=1, prefold=0)
+    assert rel_l2(img, ref0) < 1e-3
+
+
+def test_pair_counter(cuda, ktm_lib):
+    import torch
+    import ktm
+    # traces long enough that the end-of-trace cull never fires
+    case = random_case(5, ntr=64, nt=4000, nx=4, ny=4, nz=96)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    cnt = torch.zeros(1, dtype=torch.int64, device=cuda)
+    fast(cuda, case, pick="linear", pairs_counter=cnt)
+    assert int(cnt.item()) == gx.imagePnts * gy.imagePnts * gz.imagePnts * len(mx)
+    cnt.zero_()
+    fast(cuda, case, pick="linear", aperture=150.0, pairs_counter=cnt)
+    assert int(cnt.item()) == oracle.count_aperture_pairs(gx, gy, gz, mx, my, 150.0)
+
+
+def test_fast_host_and_device_paths_identical(cuda, ktm_lib):
+    import ktm
+    case = random_case(8, ntr=70, nz=150)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    dev = fast(cuda, case, pick="linear", aperture=250.0)
+    host = ktm.migrate(imageX=gx, imageY=gy, imageZ=gz, dt=dt, midX=mx, midY=my, offX=ox, offY=oy,
+                       traces=tr, velocity=vel, pick="linear", aperture=250.0)
+    assert np.array_equal(dev, host)
+
+
+@pytest.mark.parametrize("tile_run", [256, 384, 512])
+def test_fast_tile_runs_agree(cuda, ktm_lib, tile_run):
+    case = random_case(9, ntr=33, nz=700)
+    a = fast(cuda, case, pick="linear", tile_run=tile_run)
+    ref = oracle.migrate_f64(*case, pick=1, prefold=1)
+    assert rel_l2(a, ref) < 2e-5
+
+
+def test_f64_device_matches_cpu_oracle(cuda, ktm_lib):
+    import torch
+    import ktm
+    case = random_case(10, ntr=60, nx=4, ny=3, nz=120)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    cols = torch.tensor([0, 5, 11, 7], dtype=torch.int32)
+    out = ktm.migrate_columns_f64(columns=cols, imageX=gx, imageY=gy, imageZ=gz, dt=dt,
+                                  midX=_t(mx, cuda), midY=_t(my, cuda), offX=_t(ox, cuda),
+                                  offY=_t(oy, cuda), traces=_t(tr, cuda), velocity=_t(vel, cuda),
+                                  pick="linear", aperture=260.0).cpu().numpy()
+    full = oracle.migrate_f64(*case, pick=1, aperture=260.0).reshape(-1, gz.imagePnts)
+    assert np.allclose(out, full[cols.numpy()], rtol=1e-10, atol=1e-10 * np.abs(full).max())
