@@ -127,11 +127,14 @@ typedef struct ktm_job {
     const float* offX;                         /* half offsets */
     const float* offY;
     const void*  traces;                       /* [traceNo][traceStride] in traceFormat */
-    const float* traceScale;                   /* [traceNo] for F16/BF16 (NULL: 1.0) */
+    const float* traceScale;                   /* [traceNo] multiplier (NULL: 1.0) */
     int   traceFormat;                         /* KTM_FMT_* */
     int   traceStride;                         /* samples between traces; 0 = tracePts */
-    int   tracesPrefolded;                     /* 1: samples already carry sqrt(j*dt)
-                                                  (ktmPrepareTraces weightPrefold=1) */
+    int   tracesPacked;                        /* 1: traces come from ktmPrepareTraces
+                                                  (traceStride = its pitch, zero guard
+                                                  samples at 0 and >= tracePts) */
+    int   tracesPrefolded;                     /* 1: packed samples carry sqrt(j*dt)
+                                                  (ktmPrepareTraces prefold = 1) */
     const float* velocity;                     /* m/s: [Nz], or [Nx][Ny][Nz] if velocityCube */
     int   velocityCube;
     float* image;                              /* [Nx][Ny][Nz] */
@@ -160,6 +163,49 @@ size_t ktmJobStructSize(void);
  * synchronous when host buffers are given.  Replaces the body of
  * ktmMigrationCPU (psktmCPU.c:56-90) with the extended method. */
 int ktmMigrate(const ktm_job* job);
+
+/* ------------------------------------------------------------------------ */
+/* Trace preparation: rho pre-filter, weight fold, quantisation, packing    */
+/* ------------------------------------------------------------------------ */
+
+/* Rho filter options of ktmApplyRhoFilter.m (:39-58). */
+enum {
+    KTM_RHO_NONE = 0,
+    KTM_RHO_2D = 1,         /* |omega| */
+    KTM_RHO_25D = 2,        /* sqrt|omega| exp(i pi/4 sign omega) */
+    KTM_RHO_3D = 3          /* i omega */
+};
+
+typedef struct ktm_prep {
+    int   traceNo, tracePts;
+    int   inStride;            /* samples between input traces (0: tracePts) */
+    float sampleRate;          /* s */
+    const float* in;           /* F32 [traceNo][inStride], device memory */
+    int   rho;                 /* KTM_RHO_*: the rho filter of ktmApplyRhoFilter.m:22-62
+                                  (FFT length 2^ceil(log2 tracePts), omega = 2 pi k / dt
+                                  with the script's scaling), applied per trace */
+    int   rhoScriptOrder;      /* 1: also reproduce the script's trace rotation for an odd
+                                  traceNo (Octave fftshift of a matrix shifts the trace
+                                  axis too): output trace q = filtered input (q+1) mod n */
+    int   prefold;             /* 1: multiply sample j by sqrt(j*dt) (the migration weight
+                                  sqrt(t), moved from every pair to every sample) */
+    int   outFormat;           /* KTM_FMT_F32 / F16 / BF16 */
+    int   outPitch;            /* elements per packed trace (0: ktmPackedPitch) */
+    void* out;                 /* [traceNo][outPitch], device memory, 16-byte aligned */
+    float* outScale;           /* [traceNo] per-trace scale, device memory */
+    void* stream;              /* cudaStream_t */
+} ktm_prep;
+
+/* Default pitch of a packed trace: tracePts + 2 rounded up to 16 bytes. */
+int ktmPackedPitch(int tracePts, int format);
+
+/* Filter (optional), weight (optional), quantise and pack traces for the fast
+ * migration kernel.  Packed trace k holds out[k][j] = q_j for 0 < j < tracePts
+ * and zero at j = 0 and j >= tracePts (the reference's pick window 0 < it <
+ * tracePts, psktmCPU.c:82); x_j = outScale[k] * q_j.  F16/BF16 scales put the
+ * largest |sample| of each trace at 32768 / 1.  Replaces the Octave
+ * pre-processing ktmApplyRhoFilter.m with a device step.  Asynchronous. */
+int ktmPrepareTraces(const ktm_prep* prep);
 
 /* FP64 device evaluation of the job's method (pick, aperture, Vrms cube,
  * weight) for the image columns columns[0..ncols) (column index = ix*Ny + iy;

@@ -104,15 +104,58 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
     }
     if (j->mode == KTM_MODE_FAST) {
         FastArgs a;
+        std::memset(&a, 0, sizeof(a));
         a.g = g; a.midX = midX; a.midY = midY; a.offX = offX; a.offY = offY;
-        a.traces = traces; a.scale = scale; a.fmt = j->traceFormat;
-        a.weightMode = j->tracesPrefolded ? 2 : (j->pick == KTM_PICK_LINEAR ? 1 : 0);
         a.vel = vel; a.velCube = j->velocityCube;
         a.image = image; a.accumulate = j->accumulate;
         a.pick = j->pick; a.aperture = j->aperture;
         a.tileRun = j->tileRun; a.tileCols = j->tileCols;
         a.pairsEvaluated = j->pairsEvaluated;
-        return launch_fast(a, s);
+        const int wantPrefold = j->pick == KTM_PICK_LINEAR ? 1 : 0;
+        if (j->tracesPacked) {
+            if (j->tracesPrefolded != wantPrefold)
+                return set_error(KTM_ERR_ARG, "packed traces: linear pick needs prefold = 1, "
+                                              "truncating pick prefold = 0");
+            a.traces = traces; a.scale = scale; a.fmt = j->traceFormat; a.pitch = g.stride;
+            if (!scale) return set_error(KTM_ERR_ARG, "packed traces need traceScale");
+            return launch_fast(a, s);
+        }
+        // raw traces: pack into a temporary F32 set (rho off)
+        const float* in = static_cast<const float*>(traces);
+        void* packed = nullptr;
+        float* pscale = nullptr;
+        const float* src32 = in;
+        void* widened = nullptr;
+        int rc = KTM_OK;
+        if (j->traceFormat != KTM_FMT_F32) {
+            // half-precision input: widen (times its scale) to F32 first
+            rc = widen_traces(traces, j->traceFormat, scale, g.ntr, g.nt, g.stride, &widened, s);
+            if (rc) return rc;
+            src32 = static_cast<const float*>(widened);
+        }
+        const int pitch = packed_pitch(g.nt, KTM_FMT_F32);
+        cudaError_t e = cudaMallocAsync(&packed, (size_t)g.ntr * pitch * sizeof(float), s);
+        if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&pscale), (size_t)g.ntr * 4, s);
+        if (e != cudaSuccess) {
+            rc = set_error(KTM_ERR_NOMEM, "fast path: packing buffer: %s", cudaGetErrorString(e));
+        } else {
+            ktm_prep p;
+            std::memset(&p, 0, sizeof(p));
+            p.traceNo = g.ntr; p.tracePts = g.nt;
+            p.inStride = widened ? g.nt : g.stride;
+            p.sampleRate = g.dt; p.in = src32; p.prefold = wantPrefold;
+            p.outFormat = KTM_FMT_F32; p.outPitch = pitch; p.out = packed; p.outScale = pscale;
+            p.stream = s;
+            rc = prepare_traces(&p);
+            if (!rc) {
+                a.traces = packed; a.scale = pscale; a.fmt = KTM_FMT_F32; a.pitch = pitch;
+                rc = launch_fast(a, s);
+            }
+        }
+        if (packed) cudaFreeAsync(packed, s);
+        if (pscale) cudaFreeAsync(pscale, s);
+        if (widened) cudaFreeAsync(widened, s);
+        return rc;
     }
     return set_error(KTM_ERR_ARG, "ktmMigrate: mode must be REFERENCE or FAST "
                                   "(FP64 output goes through ktmMigrateColumnsF64)");
@@ -281,7 +324,7 @@ int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, doub
     ktm::FastArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g = g; a.midX = job->midX; a.midY = job->midY; a.offX = job->offX; a.offY = job->offY;
-    a.traces = job->traces; a.scale = job->traceScale; a.fmt = job->traceFormat;
+    a.traces = job->traces; a.scale = job->traceScale; a.fmt = job->traceFormat; a.pitch = g.stride;
     a.weightMode = job->tracesPrefolded ? 2 : 0;
     a.vel = job->velocity; a.velCube = job->velocityCube;
     a.pick = job->pick; a.aperture = job->aperture;

@@ -1,31 +1,38 @@
 // ktm_fast.cu -- the fast PSTM gather kernel (mixed precision) and the FP64
 // device reference.
 //
-// Method (same as psktmCPU.c:56-86, extended as the north star asks):
-//   image[x,tau] = |tau| * sum_k  w_k(t) * pick(trace_k, t/dt)
+// Method (psktmCPU.c:56-86, extended as the north star asks):
+//   image[x,tau] = |tau| * sum_k  s_k * w(t) * pick(q_k, t/dt)
 //   t = sqrt(tau^2 + |s-x|^2 S) + sqrt(tau^2 + |r-x|^2 S),  S = 1/v(x,tau)^2
-//   w = sqrt(t)  (the reference weight t*sqrt(tau^2/t) = |tau| sqrt(t), :85)
-//   pick = linear interpolation (or truncation, :80), samples outside
-//   0 < j < tracePts read as zero (:82); pairs with |mid - x| > aperture skipped.
+//   reference weight t*sqrt(tau^2/t) = |tau| sqrt(t) (:85): |tau| per image
+//   sample, sqrt(t) per pair (truncating pick) or folded into the samples as
+//   sqrt(j dt) by ktmPrepareTraces (linear pick);
+//   pick: linear interpolation, or truncation (:80); samples outside
+//   0 < j < tracePts are zero guards of the packed layout (:82);
+//   pairs with |mid - x| > aperture are skipped.
 //
-// Arithmetic per (image sample, trace) pair, everything in FP32:
-//   a_s = T2' + Ds*S', a_r = T2' + Dr*S'   (T2' = (tau/dt)^2, S' = S/dt^2:
-//                                           the traveltime comes out in samples)
-//   u   = sqrt.approx(a_s) + sqrt.approx(a_r)          2 SFU ops
-//   u   = min(u, nt)   (also maps NaN to nt: reads the zero guard sample)
-//   i0  = floor(u) by the round-down 1.5*2^23 add, f = u - i0
-//   (d, dd) = stage[i0]  (float2: sample and forward difference)
-//   acc += d + f*dd                               (prefolded weight)
-//   acc += sqrt.approx(u) * (d + f*dd)            (in-kernel weight, 3rd SFU op)
-// The per-trace FP32 scale (F16/BF16 storage) and, when prefolded, sqrt(j*dt)
-// are multiplied into the staged samples once per CTA, not once per pair.
+// Input: a PACKED trace set (ktm_prep.cu): [traceNo][pitch] F32/F16/BF16 with
+// zero guard samples, a per-trace FP32 scale s_k.
 //
-// Work decomposition: CTA = kWarps warps, warp w = one image column x a run
-// of 32*R tau samples (lane L owns tau = run0 + L + 32 r), one run per CTA
-// (blockIdx.y).  Per chunk of traces the CTA computes, for every (trace,
-// column) pair, the squared source/receiver distances and a skip flag
-// (aperture, or a lower bound on u over the run beyond the trace end), so the
-// inner loop branches once per trace, warp-uniformly.
+// Per (image sample, trace) pair, FP32 with two pairs per packed f32x2 op:
+//   a_s = T2' + Ds*S', a_r = T2' + Dr*S'  (T2' = (tau/dt)^2, S' = S/dt^2, so
+//                                          the traveltime comes out in samples)
+//   u   = sqrt(a_s) + sqrt(a_r)           2 SFU ops (sqrt.approx)
+//   u   = min(u, nt)   (also maps NaN to nt, a zero guard)
+//   i0  = floor(u) via the round-down add of 1.5*2^23, f = u - i0
+//   v   = q[i0] + f (q[i0+1] - q[i0]);  acc += s_k * v
+// Work decomposition (148 SMs, two 8-warp CTAs per SM):
+//   warp   = one image column x a run of 32*R tau samples (lane L owns
+//            tau = run0 + L + 32 r): a warp reads a narrow window of a trace;
+//   CTA    = 8 columns (blockIdx.x) x one run (blockIdx.y) x one slice of the
+//            traces (blockIdx.z); slices write partial images that a second
+//            kernel sums in a fixed order (deterministic), so small images still
+//            fill the GPU;
+//   traces stream through shared memory in chunks, double-buffered with
+//   16-byte cp.async; for each chunk the CTA first computes per (trace,
+//   column) the squared distances and a skip flag (aperture, or a lower bound
+//   of u over the run beyond the trace end), so the inner loop branches once
+//   per trace, warp-uniformly.
 #include "ktm_internal.cuh"
 
 #include <cuda_bf16.h>
@@ -38,6 +45,52 @@ constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
+constexpr size_t kFastSmemBudget = 110 * 1024;   // two CTAs per SM
+
+// ------------------------------------------------------------- f32x2 PTX ---
+struct f2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ f2 pk(float a, float b)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk(f2 x, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ f2 add2_rm(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b)
+{
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
 
 __device__ __forceinline__ float sqrt_approx(float x)
 {
@@ -46,30 +99,72 @@ __device__ __forceinline__ float sqrt_approx(float x)
     return y;
 }
 
-__device__ __forceinline__ float load_sample(const void* p, int fmt, size_t idx)
+// packed sample element -> float
+template <int FMT> struct Elem;
+template <> struct Elem<KTM_FMT_F32> {
+    using T = float;
+    static __device__ __forceinline__ float get(const T* p, int i) { return p[i]; }
+};
+template <> struct Elem<KTM_FMT_BF16> {
+    using T = unsigned short;
+    static __device__ __forceinline__ float get(const T* p, int i)
+    {
+        return __uint_as_float(static_cast<unsigned>(p[i]) << 16);
+    }
+};
+template <> struct Elem<KTM_FMT_F16> {
+    using T = __half;
+    static __device__ __forceinline__ float get(const T* p, int i) { return __half2float(p[i]); }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 {
-    if (fmt == KTM_FMT_F32) return static_cast<const float*>(p)[idx];
-    if (fmt == KTM_FMT_F16) return __half2float(static_cast<const __half*>(p)[idx]);
-    return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[idx]);
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n"); }
 
 struct ColInfo {
     float x, y;       // column coordinates
     float t2min;      // min over the run of (tau/dt)^2
-    float smin;       // min over the run of S' = 1/(v dt)^2
+    float smin;       // min over the run of S' = 1/(v dt)^2; < 0: column outside the image
 };
 
-template <int R, int PICK, int PREFOLD>
-__global__ void __launch_bounds__(kThreads, 2)
-fast_kernel(FastArgs a, int chunk, int ns)
+struct ChunkSmem {
+    // layout of one CTA's dynamic shared memory
+    size_t rawBytes, crdOff, geoOff, total;
+};
+
+__host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize)
 {
+    ChunkSmem L;
+    L.rawBytes = (size_t)chunk * pitch * esize;              // one buffer
+    L.crdOff = 2 * L.rawBytes;                               // [2][5][chunk] floats
+    L.geoOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
+    L.total = L.geoOff + (size_t)chunk * kWarps * sizeof(float4);
+    return L;
+}
+
+template <int R, int PICK, int FMT>
+__global__ void __launch_bounds__(kThreads, 2)
+fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
+{
+    static_assert(R % 2 == 0, "R pairs");
+    using T = typename Elem<FMT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* stage = reinterpret_cast<float2*>(smem_raw);                 // [chunk][ns]
-    float2* geo = stage + (size_t)chunk * ns;                            // [chunk][kWarps]
-    float* wtab = reinterpret_cast<float*>(geo + chunk * kWarps);        // [ns] sqrt(j*dt)
+    const Geometry& g = a.g;
+    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T));
+    T* rawBase = reinterpret_cast<T*>(smem_raw);
+    float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
+    float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
     __shared__ ColInfo cinfo[kWarps];
 
-    const Geometry& g = a.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ncols = g.nx * g.ny;
     const int col = blockIdx.x * kWarps + warp;
@@ -78,23 +173,28 @@ fast_kernel(FastArgs a, int chunk, int ns)
     const int run0 = blockIdx.y * (32 * R);
     const float invdt = 1.0f / g.dt;
 
-    // ---- per-thread tau tables -------------------------------------------
-    float T2[R], S[R], acc[R];
+    // ---- per-thread tau tables, two tau samples per packed register pair ----
+    f2 T2[R / 2], S2[R / 2], acc[R / 2];
     float t2min = 3.0e38f, smin = 3.0e38f;
     int nvalid = 0;
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-        int l = run0 + lane + 32 * r;
-        bool ok = l < g.nz;
-        int lc = ok ? l : g.nz - 1;
-        float tau = g.z0 + (float)lc * g.dz;
-        float tq = tau * invdt;
-        T2[r] = tq * tq;
-        float v = a.velCube ? a.vel[(size_t)(colValid ? col : 0) * g.nz + lc] : a.vel[lc];
-        float vd = v * g.dt;
-        S[r] = 1.0f / (vd * vd);
-        acc[r] = 0.0f;
-        if (ok) { t2min = fminf(t2min, T2[r]); smin = fminf(smin, S[r]); nvalid++; }
+    for (int h = 0; h < R / 2; h++) {
+        float tv[2], sv[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int l = run0 + lane + 32 * (2 * h + e);
+            const bool ok = l < g.nz;
+            const int lc = ok ? l : g.nz - 1;
+            const float tq = (g.z0 + (float)lc * g.dz) * invdt;
+            const float v = a.velCube ? a.vel[(size_t)(colValid ? col : 0) * g.nz + lc] : a.vel[lc];
+            const float vd = v * g.dt;
+            tv[e] = tq * tq;
+            sv[e] = 1.0f / (vd * vd);
+            if (ok) { t2min = fminf(t2min, tv[e]); smin = fminf(smin, sv[e]); nvalid++; }
+        }
+        T2[h] = pk(tv[0], tv[1]);
+        S2[h] = pk(sv[0], sv[1]);
+        acc[h] = pk(0.0f, 0.0f);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -106,145 +206,216 @@ fast_kernel(FastArgs a, int chunk, int ns)
         cinfo[warp].x = g.x0 + (float)ci * g.dx;
         cinfo[warp].y = g.y0 + (float)cj * g.dy;
         cinfo[warp].t2min = t2min;
-        cinfo[warp].smin = colValid ? smin : -1.0f;    // -1: column outside the image
+        cinfo[warp].smin = colValid ? smin : -1.0f;
     }
-    if (PREFOLD && a.weightMode == 1) {
-        for (int j = threadIdx.x; j < ns; j += kThreads) wtab[j] = sqrtf((float)j * g.dt);
-    }
-    __syncthreads();
+
+    const int kb = blockIdx.z * perSlice;
+    const int ke = min(g.ntr, kb + perSlice);
+    const int nchunks = ke > kb ? (ke - kb + chunk - 1) / chunk : 0;
+    const size_t rowBytes = (size_t)a.pitch * sizeof(T);
+
+    auto issue = [&](int ch) {
+        const int k0 = kb + ch * chunk, n = min(chunk, ke - k0);
+        const int b = ch & 1;
+        unsigned char* dst = reinterpret_cast<unsigned char*>(rawBase) + b * L.rawBytes;
+        const unsigned char* src = static_cast<const unsigned char*>(a.traces) + (size_t)k0 * rowBytes;
+        const int pieces = (int)((size_t)n * rowBytes / 16);
+        for (int q = threadIdx.x; q < pieces; q += kThreads) cp_async16(dst + 16 * (size_t)q, src + 16 * (size_t)q);
+        float* crd = crdBase + b * 5 * chunk;
+        for (int q = threadIdx.x; q < 5 * n; q += kThreads) {
+            const int arr = q / n, c = q % n;
+            const float* srcArr = arr == 0 ? a.midX : arr == 1 ? a.midY : arr == 2 ? a.offX
+                                : arr == 3 ? a.offY : a.scale;
+            cp_async4(crd + arr * chunk + c, srcArr + k0 + c);
+        }
+        cp_async_commit();
+    };
 
     const float umax = (float)g.nt;
     const float ap2 = a.aperture > 0.0f ? a.aperture * a.aperture : -1.0f;
+    const f2 M2 = pk(kMagic, kMagic);
     unsigned long long evaluated = 0;
 
-    const int nchunks = (g.ntr + chunk - 1) / chunk;
+    if (nchunks > 0) issue(0);
     for (int ch = 0; ch < nchunks; ch++) {
-        const int k0 = ch * chunk, n = min(chunk, g.ntr - k0);
-        // ---- stage samples: (d_j, d_{j+1} - d_j), j = 0..nt, zero guards --
-        for (int c = 0; c < n; c++) {
-            const size_t base = (size_t)(k0 + c) * g.stride;
-            const float sc = a.scale ? a.scale[k0 + c] : 1.0f;
-            float2* dst = stage + (size_t)c * ns;
-            for (int j = threadIdx.x; j < ns; j += kThreads) {
-                float d0 = 0.0f, d1 = 0.0f;
-                if (j > 0 && j < g.nt) d0 = load_sample(a.traces, a.fmt, base + j) * sc;
-                if (j + 1 < g.nt) d1 = load_sample(a.traces, a.fmt, base + j + 1) * sc;
-                if (PREFOLD && a.weightMode == 1) {
-                    d0 *= (j > 0 && j < g.nt) ? wtab[j] : 0.0f;
-                    d1 *= (j + 1 < g.nt) ? wtab[j + 1] : 0.0f;
+        const int b = ch & 1;
+        const int k0 = kb + ch * chunk, n = min(chunk, ke - k0);
+        cp_async_wait_all();
+        __syncthreads();                       // chunk ch landed; chunk ch-1 fully consumed
+        if (ch + 1 < nchunks) issue(ch + 1);
+        // ---- per (trace, column) distances, scale and skip flag --------------
+        {
+            const float* crd = crdBase + b * 5 * chunk;
+            for (int p = threadIdx.x; p < chunk * kWarps; p += kThreads) {
+                const int c = p / kWarps, w = p % kWarps;
+                float4 gd = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+                const ColInfo cw = cinfo[w];
+                if (c < n && cw.smin >= 0.0f) {
+                    const float mx = crd[c], my = crd[chunk + c], ox = crd[2 * chunk + c],
+                                oy = crd[3 * chunk + c], sc = crd[4 * chunk + c];
+                    const float dmx = mx - cw.x, dmy = my - cw.y;
+                    const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
+                    const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
+                    bool keep = !(ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2);
+                    if (keep) {
+                        // lower bound of u over the run: past the last sample -> no contribution
+                        const float ulb = sqrtf(fmaf(ds, cw.smin, cw.t2min)) +
+                                          sqrtf(fmaf(dr, cw.smin, cw.t2min));
+                        keep = ulb < umax * 1.0001f + 1.0f;
+                    }
+                    if (keep) gd = make_float4(ds, dr, sc, 0.0f);
                 }
-                dst[j] = make_float2(d0, d1 - d0);
+                geo[p] = gd;
             }
-        }
-        // ---- per (trace, column) distances and skip flags ------------------
-        for (int p = threadIdx.x; p < chunk * kWarps; p += kThreads) {
-            const int c = p / kWarps, w = p % kWarps;
-            float2 gd = make_float2(-1.0f, 0.0f);
-            const ColInfo ciw = cinfo[w];
-            if (c < n && ciw.smin >= 0.0f) {
-                const int k = k0 + c;
-                const float mx = a.midX[k], my = a.midY[k], ox = a.offX[k], oy = a.offY[k];
-                const float dmx = mx - ciw.x, dmy = my - ciw.y;
-                const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
-                const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
-                bool keep = !(ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2);
-                if (keep) {
-                    // lower bound of u over the run; beyond the last sample -> no contribution
-                    float ulb = sqrtf(fmaf(ds, ciw.smin, ciw.t2min)) +
-                                sqrtf(fmaf(dr, ciw.smin, ciw.t2min));
-                    keep = ulb < umax * 1.0001f + 1.0f;
-                }
-                if (keep) gd = make_float2(ds, dr);
-            }
-            geo[p] = gd;
         }
         __syncthreads();
-
         if (colValid) {
-            const float2* gw = geo + warp;
+            const T* rows = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(rawBase) +
+                                                       b * L.rawBytes);
             for (int c = 0; c < n; c++) {
-                const float2 gd = gw[c * kWarps];
+                const float4 gd = geo[c * kWarps + warp];
                 if (gd.x < 0.0f) continue;                 // warp-uniform
                 evaluated += nvalid;
-                const float2* tr = stage + (size_t)c * ns;
+                const T* row = rows + (size_t)c * a.pitch;
+                const f2 DS = pk(gd.x, gd.x), DR = pk(gd.y, gd.y), SC = pk(gd.z, gd.z);
 #pragma unroll
-                for (int r = 0; r < R; r++) {
-                    float as = fmaf(gd.x, S[r], T2[r]);
-                    float ar = fmaf(gd.y, S[r], T2[r]);
-                    float u = sqrt_approx(as) + sqrt_approx(ar);
-                    u = fminf(u, umax);
-                    float fl = __fadd_rd(u, kMagic);
-                    int i0 = __float_as_int(fl) - kMagicBits;
-                    float2 dd = tr[i0];
+                for (int h = 0; h < R / 2; h++) {
+                    float as0, as1, ar0, ar1;
+                    upk(fma2(DS, S2[h], T2[h]), as0, as1);
+                    upk(fma2(DR, S2[h], T2[h]), ar0, ar1);
+                    f2 U = add2(pk(sqrt_approx(as0), sqrt_approx(as1)),
+                                pk(sqrt_approx(ar0), sqrt_approx(ar1)));
+                    float u0, u1;
+                    upk(U, u0, u1);
+                    u0 = fminf(u0, umax);
+                    u1 = fminf(u1, umax);
+                    U = pk(u0, u1);
+                    const f2 FL = add2_rm(U, M2);
+                    float fl0, fl1;
+                    upk(FL, fl0, fl1);
+                    const int i0 = __float_as_int(fl0) - kMagicBits;
+                    const int i1 = __float_as_int(fl1) - kMagicBits;
+                    const float a0 = Elem<FMT>::get(row, i0), a1 = Elem<FMT>::get(row, i1);
                     if (PICK == KTM_PICK_LINEAR) {
-                        float f = u - (fl - kMagic);
-                        float v = fmaf(f, dd.y, dd.x);
-                        if (PREFOLD) acc[r] += v;
-                        else acc[r] = fmaf(sqrt_approx(u), v, acc[r]);
+                        const float b0 = Elem<FMT>::get(row, i0 + 1), b1 = Elem<FMT>::get(row, i1 + 1);
+                        const f2 F = sub2(U, sub2(FL, M2));
+                        const f2 A = pk(a0, a1);
+                        const f2 V = fma2(F, sub2(pk(b0, b1), A), A);
+                        acc[h] = fma2(SC, V, acc[h]);
                     } else {
-                        if (PREFOLD) acc[r] += dd.x;
-                        else acc[r] = fmaf(sqrt_approx(u), dd.x, acc[r]);
+                        // weight sqrt(t) per pair (u in samples; sqrt(dt) applied at the end)
+                        const f2 W = mul2(SC, pk(sqrt_approx(u0), sqrt_approx(u1)));
+                        acc[h] = fma2(W, pk(a0, a1), acc[h]);
                     }
                 }
             }
         }
-        __syncthreads();
     }
 
     if (colValid) {
-        // weight factor |tau| (and sqrt(dt): in-kernel weight used u = t/dt)
-        const float wscale = PREFOLD ? 1.0f : sqrtf(g.dt);
-        float* out = a.image + (size_t)col * g.nz;
+        const float wscale = PICK == KTM_PICK_LINEAR ? 1.0f : sqrtf(g.dt);
+        const size_t nimg = (size_t)ncols * g.nz;
+        float* out = partial ? partial + blockIdx.z * nimg + (size_t)col * g.nz
+                             : a.image + (size_t)col * g.nz;
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            int l = run0 + lane + 32 * r;
-            if (l < g.nz) {
-                float tau = fabsf(g.z0 + (float)l * g.dz);
-                float v = acc[r] * (tau * wscale);
-                out[l] = a.accumulate ? out[l] + v : v;
+        for (int h = 0; h < R / 2; h++) {
+            float v2[2];
+            upk(acc[h], v2[0], v2[1]);
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int l = run0 + lane + 32 * (2 * h + e);
+                if (l < g.nz) {
+                    const float tau = fabsf(g.z0 + (float)l * g.dz);
+                    const float v = v2[e] * (tau * wscale);
+                    out[l] = (!partial && a.accumulate) ? out[l] + v : v;
+                }
             }
         }
     }
-    if (a.pairsEvaluated) {
-        // every lane of a warp counted the same pairs; lane 0 reports the warp's
-        if (lane == 0 && evaluated) atomicAdd(a.pairsEvaluated, evaluated);
+    if (a.pairsEvaluated && lane == 0 && evaluated) atomicAdd(a.pairsEvaluated, evaluated);
+}
+
+// out[i] = (accumulate ? out[i] : 0) + sum_z partial[z][i], z in increasing order
+__global__ void reduce_slices(float* __restrict__ out, const float* __restrict__ partial,
+                              size_t nimg, int nslices, int accumulate)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nimg;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float s = accumulate ? out[i] : 0.0f;
+        for (int z = 0; z < nslices; z++) s += partial[(size_t)z * nimg + i];
+        out[i] = s;
     }
 }
 
-template <int R, int PICK, int PREFOLD>
-int launch_t(const FastArgs& a, cudaStream_t stream)
+template <int R, int PICK, int FMT>
+int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const Geometry& g = a.g;
-    const int ns = g.nt + 1;
-    const size_t perTrace = (size_t)ns * sizeof(float2) + kWarps * sizeof(float2);
-    const size_t fixed = (size_t)ns * sizeof(float) + 64;
-    // two CTAs per SM: about 113 KB each
-    const size_t budget = 112 * 1024;
-    int chunk = budget > fixed ? (int)((budget - fixed) / perTrace) : 0;
-    if (chunk < 1) chunk = (int)((kMaxSmemBytes - fixed) / perTrace);
-    if (chunk < 1)
-        return set_error(KTM_ERR_LIMIT,
-                         "fast kernel: tracePts=%d exceeds the shared-memory stage limit", g.nt);
-    if (chunk > 32) chunk = 32;
-    const size_t smem = fixed + (size_t)chunk * perTrace;
-    auto kern = fast_kernel<R, PICK, PREFOLD>;
-    KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+    const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
+    int chunk = 32;
+    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize).total > kFastSmemBudget) chunk--;
+    if (chunk_layout(chunk, a.pitch, esize).total > (size_t)kMaxSmemBytes)
+        return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
+                                        "stage limit", a.pitch);
+    const size_t smem = chunk_layout(chunk, a.pitch, esize).total;
+    auto kern = fast_kernel<R, PICK, FMT>;
+    KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
     const long long cols = (long long)g.nx * g.ny;
-    dim3 grid((unsigned)((cols + kWarps - 1) / kWarps), (unsigned)((g.nz + 32 * R - 1) / (32 * R)));
-    kern<<<grid, kThreads, smem, stream>>>(a, chunk, ns);
-    KTM_CUDA_TRY(cudaGetLastError());
+    const unsigned gx = (unsigned)((cols + kWarps - 1) / kWarps);
+    const unsigned gy = (unsigned)((g.nz + 32 * R - 1) / (32 * R));
+    if (gy > 65535) return set_error(KTM_ERR_LIMIT, "fast kernel: Nz too large");
+    // trace slices: enough CTAs for about four waves of two CTAs per SM, each
+    // slice keeping at least four chunks of traces
+    const long long base = (long long)gx * gy;
+    const long long want = 8LL * smCount;
+    int slices = (int)((want + base - 1) / base);
+    const int maxSlices = max(1, g.ntr / (4 * chunk));
+    slices = max(1, min(slices, min(maxSlices, 64)));
+    if (a.slices > 0) slices = min(a.slices, max(1, g.ntr));
+    const int perSlice = (g.ntr + slices - 1) / slices;
+    slices = (g.ntr + perSlice - 1) / perSlice;
+
+    float* partial = nullptr;
+    const size_t nimg = (size_t)cols * g.nz;
+    if (slices > 1) {
+        if (a.scratch && a.scratchBytes >= (size_t)slices * nimg * sizeof(float)) {
+            partial = static_cast<float*>(a.scratch);
+        } else {
+            KTM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&partial),
+                                         (size_t)slices * nimg * sizeof(float), stream));
+        }
+    }
+    dim3 grid(gx, gy, (unsigned)slices);
+    kern<<<grid, kThreads, smem, stream>>>(a, chunk, perSlice, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && partial) {
+        const int th = 256;
+        const size_t want = (nimg + th - 1) / th, cap = (size_t)smCount * 8;
+        const unsigned blocks = (unsigned)(want < cap ? want : cap);
+        reduce_slices<<<blocks, th, 0, stream>>>(a.image, partial, nimg, slices, a.accumulate);
+        e = cudaGetLastError();
+    }
+    if (partial && partial != a.scratch) cudaFreeAsync(partial, stream);
+    if (e != cudaSuccess) return set_error(KTM_ERR_CUDA, "fast kernel launch: %s", cudaGetErrorString(e));
     return KTM_OK;
 }
 
-template <int R>
-int launch_pick(const FastArgs& a, cudaStream_t stream)
+template <int R, int PICK>
+int launch_fmt(const FastArgs& a, cudaStream_t s, int sm)
 {
-    if (a.pick == KTM_PICK_LINEAR)
-        return a.weightMode ? launch_t<R, KTM_PICK_LINEAR, 1>(a, stream)
-                            : launch_t<R, KTM_PICK_LINEAR, 0>(a, stream);
-    return a.weightMode ? launch_t<R, KTM_PICK_TRUNCATE, 1>(a, stream)
-                        : launch_t<R, KTM_PICK_TRUNCATE, 0>(a, stream);
+    switch (a.fmt) {
+        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32>(a, s, sm);
+        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16>(a, s, sm);
+        default: return launch_t<R, PICK, KTM_FMT_BF16>(a, s, sm);
+    }
+}
+
+template <int R>
+int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
+{
+    return a.pick == KTM_PICK_LINEAR ? launch_fmt<R, KTM_PICK_LINEAR>(a, s, sm)
+                                     : launch_fmt<R, KTM_PICK_TRUNCATE>(a, s, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -252,6 +423,13 @@ int launch_pick(const FastArgs& a, cudaStream_t stream)
 // global memory.  Slow; used to measure the error of the fast path on
 // configurations too large for the CPU oracle.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double load_any(const void* p, int fmt, size_t idx)
+{
+    if (fmt == KTM_FMT_F32) return (double)static_cast<const float*>(p)[idx];
+    if (fmt == KTM_FMT_F16) return (double)__half2float(static_cast<const __half*>(p)[idx]);
+    return (double)__bfloat162float(static_cast<const __nv_bfloat16*>(p)[idx]);
+}
+
 __global__ void f64_kernel(FastArgs a, const int* __restrict__ cols, int ncols,
                            double* __restrict__ out)
 {
@@ -271,6 +449,7 @@ __global__ void f64_kernel(FastArgs a, const int* __restrict__ cols, int ncols,
     const double v = a.velCube ? (double)a.vel[(size_t)col * g.nz + l] : (double)a.vel[l];
     const double S = 1.0 / (v * v), tau2 = tau * tau, dt = (double)g.dt;
     const double ap2 = a.aperture > 0.0f ? (double)a.aperture * (double)a.aperture : -1.0;
+    const int stride = a.pitch;
     double acc = 0.0;
     for (int k = 0; k < g.ntr; k++) {
         const double mx = a.midX[k], my = a.midY[k], ox = a.offX[k], oy = a.offY[k];
@@ -281,14 +460,14 @@ __global__ void f64_kernel(FastArgs a, const int* __restrict__ cols, int ncols,
         const double u = t / dt;
         if (!(u < (double)g.nt)) continue;
         const double sc = a.scale ? (double)a.scale[k] : 1.0;
-        const size_t base = (size_t)k * g.stride;
+        const size_t base = (size_t)k * stride;
         double val;
         if (a.pick == KTM_PICK_LINEAR) {
             const double fl = floor(u);
             const int i0 = (int)fl;
             const double f = u - fl;
-            double d0 = (i0 > 0 && i0 < g.nt) ? (double)load_sample(a.traces, a.fmt, base + i0) : 0.0;
-            double d1 = (i0 + 1 > 0 && i0 + 1 < g.nt) ? (double)load_sample(a.traces, a.fmt, base + i0 + 1) : 0.0;
+            double d0 = (i0 > 0 && i0 < g.nt) ? load_any(a.traces, a.fmt, base + i0) : 0.0;
+            double d1 = (i0 + 1 > 0 && i0 + 1 < g.nt) ? load_any(a.traces, a.fmt, base + i0 + 1) : 0.0;
             if (a.weightMode == 1) {
                 d0 *= sqrt((double)i0 * dt);
                 d1 *= sqrt((double)(i0 + 1) * dt);
@@ -296,7 +475,7 @@ __global__ void f64_kernel(FastArgs a, const int* __restrict__ cols, int ncols,
             val = (1.0 - f) * d0 + f * d1;
         } else {
             const int it = (int)u;
-            val = (it > 0 && it < g.nt) ? (double)load_sample(a.traces, a.fmt, base + it) : 0.0;
+            val = (it > 0 && it < g.nt) ? load_any(a.traces, a.fmt, base + it) : 0.0;
             if (a.weightMode == 1) val *= sqrt((double)it * dt);
         }
         const double w = a.weightMode ? fabs(tau) : (t > 0.0 ? t * sqrt(tau2 / t) : 0.0);
@@ -311,33 +490,38 @@ int launch_fast(const FastArgs& a, cudaStream_t stream)
 {
     const Geometry& g = a.g;
     if ((long long)g.nx * g.ny * g.nz == 0) return KTM_OK;
-    if (g.nt >= (1 << 22))
-        return set_error(KTM_ERR_LIMIT, "fast kernel: tracePts must be < 4194304");
+    if (g.nt >= (1 << 22)) return set_error(KTM_ERR_LIMIT, "fast kernel: tracePts must be < 4194304");
     if (g.ntr == 0) {
         if (!a.accumulate)
-            KTM_CUDA_TRY(cudaMemsetAsync(a.image, 0, sizeof(float) * (size_t)g.nx * g.ny * g.nz,
-                                         stream));
+            KTM_CUDA_TRY(cudaMemsetAsync(a.image, 0, sizeof(float) * (size_t)g.nx * g.ny * g.nz, stream));
         return KTM_OK;
     }
+    const int esize = a.fmt == KTM_FMT_F32 ? 4 : 2;
+    if (a.pitch < g.nt + 2 || ((size_t)a.pitch * esize) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(a.traces) % 16 != 0)
+        return set_error(KTM_ERR_ARG, "fast kernel: traces must be a packed set (pitch >= tracePts+2, "
+                                      "16-byte rows, 16-byte aligned)");
+    int dev = 0, sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
     int R = a.tileRun > 0 ? a.tileRun / 32 : 0;
     if (R == 0) {
         int best = 16, bestWaste = 1 << 30;
         for (int r : {16, 12, 8}) {
-            int run = 32 * r, waste = ((g.nz + run - 1) / run) * run - g.nz;
+            const int run = 32 * r, waste = ((g.nz + run - 1) / run) * run - g.nz;
             if (waste < bestWaste) { bestWaste = waste; best = r; }
         }
         R = best;
     }
     switch (R) {
-        case 8: return launch_pick<8>(a, stream);
-        case 12: return launch_pick<12>(a, stream);
-        case 16: return launch_pick<16>(a, stream);
+        case 8: return launch_pick<8>(a, stream, sm);
+        case 12: return launch_pick<12>(a, stream, sm);
+        case 16: return launch_pick<16>(a, stream, sm);
         default: return set_error(KTM_ERR_ARG, "fast kernel: tileRun must be 256, 384 or 512");
     }
 }
 
-int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* out,
-                       cudaStream_t stream)
+int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* out, cudaStream_t stream)
 {
     const long long n = (long long)ncols * a.g.nz;
     if (n == 0) return KTM_OK;

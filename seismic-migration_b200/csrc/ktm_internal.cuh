@@ -48,16 +48,30 @@ struct FastArgs {
     Geometry g;
     const float* midX; const float* midY; const float* offX; const float* offY;
     const void* traces; const float* scale; int fmt;
-    // 0: weight sqrt(t) per pair; 1: sqrt(j*dt) multiplied into each staged
-    // sample; 2: stored samples already carry sqrt(j*dt)
+    int pitch;              // elements between traces
+    // FP64 reference only: 0 weight |tau| sqrt(t) per pair; 1 sqrt(j*dt) applied
+    // to each sample; 2 samples already carry sqrt(j*dt)
     int weightMode;
     const float* vel; int velCube;
     float* image; int accumulate;
     int pick; float aperture;
     int tileRun, tileCols;
+    int slices;             // trace slices (0: chosen to fill the GPU)
+    void* scratch;          // optional preallocated partial-image buffer
+    size_t scratchBytes;
     unsigned long long* pairsEvaluated;
 };
+// Fast kernel on a PACKED trace set (ktmPrepareTraces layout); linear pick
+// expects samples prefolded with sqrt(j*dt), truncating pick expects them not.
 int launch_fast(const FastArgs& a, cudaStream_t stream);
+
+// ktm_prep.cu
+int packed_pitch(int nt, int fmt);
+int prepare_traces(const ktm_prep* p);
+// F16/BF16 [ntr][stride] (times scale[k] when given) -> new F32 [ntr][nt] buffer
+// allocated stream-ordered on s (caller frees with cudaFreeAsync).
+int widen_traces(const void* in, int fmt, const float* scale, int ntr, int nt, int stride,
+                 void** out, cudaStream_t s);
 
 // FP64 device reference (ktm_fast.cu): out[q][nz] for image columns cols[q]
 // (cols == NULL: columns 0..ncols-1).

@@ -191,22 +191,40 @@ int launch_reference(const Geometry& g, const float* midX, const float* midY, co
                                          sizeof(float) * (size_t)g.nx * g.ny * g.nz, stream));
         return KTM_OK;
     }
-    // run length per warp: the R in {4, 8, 16} with the least tau padding
+    // Run length per warp.  Every image sample keeps its traces in reference
+    // order, so the traces cannot be split across CTAs; parallelism comes from
+    // the image alone: the largest R in {16, 8, 4, 2, 1} that still gives about
+    // two waves of 24 resident warps per SM, and among those the least padding.
     int R = tileRun > 0 ? tileRun / 32 : 0;
     if (R == 0) {
-        int best = 16, bestWaste = 1 << 30;
-        for (int r : {16, 8, 4}) {
-            int run = 32 * r, waste = ((g.nz + run - 1) / run) * run - g.nz;
-            if (waste < bestWaste) { bestWaste = waste; best = r; }
+        int dev = 0, sm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+        const long long cols = (long long)g.nx * g.ny;
+        const long long wantWarps = 48LL * sm;
+        R = 1;
+        for (int r : {16, 8, 4, 2}) {
+            const long long warps = cols * ((g.nz + 32 * r - 1) / (32 * r));
+            if (warps >= wantWarps) { R = r; break; }
         }
-        R = best;
+        if (R >= 8) {
+            int best = R, bestWaste = 1 << 30;
+            for (int r : {16, 8, 4}) {
+                if (r > R) continue;
+                int run = 32 * r, waste = ((g.nz + run - 1) / run) * run - g.nz;
+                if (waste < bestWaste) { bestWaste = waste; best = r; }
+            }
+            R = best;
+        }
     }
     switch (R) {
+        case 1: return launch_r<1>(g, midX, midY, offX, offY, traces, vel, image, accumulate, stream);
+        case 2: return launch_r<2>(g, midX, midY, offX, offY, traces, vel, image, accumulate, stream);
         case 4: return launch_r<4>(g, midX, midY, offX, offY, traces, vel, image, accumulate, stream);
         case 8: return launch_r<8>(g, midX, midY, offX, offY, traces, vel, image, accumulate, stream);
         case 16: return launch_r<16>(g, midX, midY, offX, offY, traces, vel, image, accumulate, stream);
         default:
-            return set_error(KTM_ERR_ARG, "reference kernel: tileRun must be 128, 256 or 512");
+            return set_error(KTM_ERR_ARG, "reference kernel: tileRun must be 32, 64, 128, 256 or 512");
     }
 }
 

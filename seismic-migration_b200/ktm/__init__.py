@@ -9,3 +9,4 @@ from ._lib import KtmError, ImageGrid, JobParams, lib, LIB_PATH  # noqa: F401
 from .api import (  # noqa: F401
     grid, ktmMigrationCPU, ktmMigrationGPU, initThreeAxes, migrate, migrate_columns_f64, Job,
 )
+from .api import PackedTraces, packed_pitch, prepare  # noqa: F401,E402

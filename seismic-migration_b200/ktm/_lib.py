@@ -59,7 +59,8 @@ class KtmJob(C.Structure):
         ("config", JobParams),
         ("midX", P), ("midY", P), ("offX", P), ("offY", P),
         ("traces", P), ("traceScale", P),
-        ("traceFormat", C.c_int), ("traceStride", C.c_int), ("tracesPrefolded", C.c_int),
+        ("traceFormat", C.c_int), ("traceStride", C.c_int), ("tracesPacked", C.c_int),
+        ("tracesPrefolded", C.c_int),
         ("velocity", P), ("velocityCube", C.c_int),
         ("image", P),
         ("mode", C.c_int), ("pick", C.c_int), ("aperture", C.c_float),
@@ -67,6 +68,16 @@ class KtmJob(C.Structure):
         ("stream", P),
         ("tileRun", C.c_int), ("tileCols", C.c_int),
         ("pairsEvaluated", P),
+    ]
+
+
+class KtmPrep(C.Structure):
+    """ktm_prep (include/ktm.h)."""
+    _fields_ = [
+        ("traceNo", C.c_int), ("tracePts", C.c_int), ("inStride", C.c_int),
+        ("sampleRate", C.c_float), ("in_", P), ("rho", C.c_int), ("rhoScriptOrder", C.c_int),
+        ("prefold", C.c_int), ("outFormat", C.c_int), ("outPitch", C.c_int), ("out", P),
+        ("outScale", P), ("stream", P),
     ]
 
 
@@ -102,6 +113,10 @@ def lib() -> C.CDLL:
     L.ktmMigrate.restype = C.c_int
     L.ktmMigrateColumnsF64.argtypes = [C.POINTER(KtmJob), P, C.c_int, P]
     L.ktmMigrateColumnsF64.restype = C.c_int
+    L.ktmPackedPitch.argtypes = [C.c_int, C.c_int]
+    L.ktmPackedPitch.restype = C.c_int
+    L.ktmPrepareTraces.argtypes = [C.POINTER(KtmPrep)]
+    L.ktmPrepareTraces.restype = C.c_int
     _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "

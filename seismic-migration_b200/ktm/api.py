@@ -28,10 +28,29 @@ def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def as_grid(g) -> ImageGrid:
+    """Any object with imagePnts / imageStep / imageStart (or a 3-tuple)."""
+    if isinstance(g, ImageGrid):
+        return g
+    if isinstance(g, (tuple, list)):
+        return ImageGrid(int(g[0]), float(g[1]), float(g[2]))
+    return ImageGrid(int(g.imagePnts), float(g.imageStep), float(g.imageStart))
+
+
+def as_params(c) -> JobParams:
+    if isinstance(c, JobParams):
+        return c
+    if isinstance(c, (tuple, list)):
+        return JobParams(int(c[0]), int(c[1]), float(c[2]))
+    return JobParams(int(c.traceNo), int(c.tracePts), float(c.traceSampleRate))
+
+
 def _dropin(fn, imageX, imageY, imageZ, config, midX, midY, offX, offY, traces, slowness,
             image=None) -> np.ndarray:
     midX, midY, offX, offY, traces, slowness = map(_f32, (midX, midY, offX, offY, traces,
                                                           slowness))
+    imageX, imageY, imageZ = map(as_grid, (imageX, imageY, imageZ))
+    config = as_params(config)
     shape = (imageX.imagePnts, imageY.imagePnts, imageZ.imagePnts)
     if image is None:
         image = np.empty(shape, np.float32)
@@ -64,6 +83,7 @@ def ktmMigrationGPU(imageX, imageY, imageZ, config, midX, midY, offX, offY, trac
 
 
 def initThreeAxes(imageX, imageY, imageZ):
+    imageX, imageY, imageZ = map(as_grid, (imageX, imageY, imageZ))
     xx = np.empty(imageX.imagePnts, np.float32)
     yy = np.empty(imageY.imagePnts, np.float32)
     zz = np.empty(imageZ.imagePnts, np.float32)
@@ -93,6 +113,65 @@ def _stream_handle(stream):
     return stream.cuda_stream
 
 
+_RHO = {None: 0, 0: 0, "none": 0, 1: 1, "2d": 1, 2: 2, "2.5d": 2, 3: 3, "3d": 3}
+
+
+class PackedTraces:
+    """A packed trace set from ``prepare`` (ktmPrepareTraces): CUDA tensor
+    [traceNo, pitch] of F32/F16/BF16 with zero guard samples, a per-trace FP32
+    scale, and whether sqrt(j*dt) is folded into the samples."""
+
+    def __init__(self, data, scale, nt: int, fmt: str, prefolded: bool, rho: int):
+        self.data, self.scale, self.nt, self.fmt = data, scale, int(nt), fmt
+        self.prefolded, self.rho = bool(prefolded), int(rho)
+
+    @property
+    def pitch(self) -> int:
+        return int(self.data.shape[1])
+
+    @property
+    def ntr(self) -> int:
+        return int(self.data.shape[0])
+
+    def unpacked(self):
+        """float32 [traceNo, nt]: scale * samples (guards dropped)."""
+        return self.data[:, : self.nt].float() * self.scale[:, None]
+
+
+def packed_pitch(nt: int, fmt: str = "bf16") -> int:
+    return int(lib().ktmPackedPitch(int(nt), _FMT[fmt]))
+
+
+def prepare(traces, dt: float, *, fmt: str = "bf16", rho=0, prefold: bool = True,
+            script_order: bool = False, stream=None, out=None, out_scale=None) -> PackedTraces:
+    """Rho filter (ktmApplyRhoFilter.m option 1/2/3), sqrt(t) weight fold,
+    per-trace scale and quantisation on the device (ktmPrepareTraces)."""
+    import torch
+    if not (_is_torch(traces) and traces.is_cuda and traces.dtype == torch.float32):
+        raise ValueError("prepare takes a CUDA float32 tensor [traceNo, tracePts]")
+    traces = traces.contiguous()
+    ntr, nt = traces.shape
+    pitch = packed_pitch(nt, fmt)
+    dtype = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[fmt]
+    if out is None:
+        out = torch.empty((ntr, pitch), device=traces.device, dtype=dtype)
+    if out_scale is None:
+        out_scale = torch.empty(ntr, device=traces.device, dtype=torch.float32)
+    p = _lib.KtmPrep()
+    p.traceNo, p.tracePts, p.inStride, p.sampleRate = ntr, nt, nt, float(dt)
+    p.in_ = traces.data_ptr()
+    p.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
+    p.rhoScriptOrder = int(bool(script_order))
+    p.prefold = int(bool(prefold))
+    p.outFormat = _FMT[fmt]
+    p.outPitch = int(out.shape[1])
+    p.out = out.data_ptr()
+    p.outScale = out_scale.data_ptr()
+    p.stream = _stream_handle(stream)
+    check(lib().ktmPrepareTraces(C.byref(p)))
+    return PackedTraces(out, out_scale, nt, fmt, prefold, p.rho)
+
+
 class Job:
     """Builds a ktm_job and keeps every array it points at alive."""
 
@@ -100,8 +179,14 @@ class Job:
                  velocity, image=None, scale=None, mode="fast", pick="linear",
                  aperture=0.0, accumulate=False, prefolded=False, fmt=None, stream=None,
                  tile_run=0, pairs_counter=None, trace_stride=0):
+        packed = None
+        if isinstance(traces, PackedTraces):
+            packed = traces
+            traces, scale, fmt = packed.data, packed.scale, packed.fmt
+            prefolded, trace_stride = packed.prefolded, packed.pitch
         dev = _is_torch(traces)
         self.device = dev
+        imageX, imageY, imageZ = map(as_grid, (imageX, imageY, imageZ))
         self.keep = []
         nx, ny, nz = imageX.imagePnts, imageY.imagePnts, imageZ.imagePnts
         if dev:
@@ -109,7 +194,7 @@ class Job:
             if not traces.is_cuda:
                 raise ValueError("torch tensors must be CUDA tensors")
             ntr = traces.shape[0]
-            nt = traces.shape[1] if trace_stride == 0 else trace_stride
+            nt = packed.nt if packed is not None else traces.shape[1]
             if fmt is None:
                 fmt = {torch.float32: "f32", torch.float16: "f16", torch.bfloat16: "bf16"}[traces.dtype]
             if image is None:
@@ -130,7 +215,7 @@ class Job:
             if image is None:
                 image = np.zeros((nx, ny, nz), np.float32)
             ntr = traces.shape[0]
-            nt = traces.shape[1] if trace_stride == 0 else trace_stride
+            nt = traces.shape[1]
         self.image = image
         self.keep += [midX, midY, offX, offY, traces, velocity, image, scale]
         j = KtmJob()
@@ -142,6 +227,7 @@ class Job:
         j.traceScale = _ptr(scale)
         j.traceFormat = _FMT[fmt]
         j.traceStride = int(trace_stride)
+        j.tracesPacked = int(packed is not None)
         j.tracesPrefolded = int(bool(prefolded))
         j.velocity = _ptr(velocity)
         j.velocityCube = int(len(velocity.shape) == 3)
