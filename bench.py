@@ -1,0 +1,436 @@
+"""Benchmark: 3-D prestack Kirchhoff time migration on B200.
+
+Workload (one GPU): a 200 x 200 x 1501 image (25 m bins, t0 at 2 ms, so tau at
+1 ms one-way) from 1,000,000 traces of 1501 samples at 2 ms; sources and
+receivers uniform over 5 x 5 km, offsets <= 4 km, uniform azimuth; Vrms
+1500 -> 4000 m/s with a seeded +-5 % lateral field (1 km correlation);
+traces = 30 Hz Ricker diffractions from 200 scatterers plus sigma 0.05 noise
+(seeded, synthesised on the device); aperture 3 km.  No public dataset exists
+for this path, so the data are synthetic with the stated shapes.
+
+A step = one batch of traces (1/16 of the survey by default) through the hot
+path: the rho pre-filter (3-D, i*omega) and FP16 packing with a per-trace
+scale (ktmPrepareTraces), then the mixed-precision
+gather kernel accumulating into the resident image (ktmMigrate).  16 steps =
+the whole job.  Each batch's traces (375 MB) exceed the 126 MB L2.
+
+Printed: one JSON line.  ``value`` = raw image-point x trace pairs per second
+of the mixed path with inputs resident in HBM; ``e2e`` = the same through the
+C ABI with host buffers (host->device copies and the image read-back inside
+the timed region); ``plain_fp32`` = the bit-exact FP32 kernel (psktmCPU.c
+arithmetic) on the same geometry; ``error`` = relative L2 / max error of one
+batch's image against the FP64 device evaluation on sampled columns;
+``cpu_baseline`` = the reference's own psktmCPU.c on this host's cores.
+
+``--impl reference`` runs the reference's CPU implementation instead
+(oracle/_ref, built from the reference sources; rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "seismic-migration_b200"))
+
+METRIC = "PSTM G(image-pt x trace)/s on 1 B200: mixed vs plain FP32 @<=1e-3 rel L2 err"
+UNIT = "Gpair/s"
+WORKLOAD = "3D PSTM 200x200x1501 image, 1e6 traces x 1501 samples @ 2 ms, aperture 3 km"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ntr", type=int, default=1_000_000)
+    ap.add_argument("--batches", type=int, default=16)
+    ap.add_argument("--fmt", default="f16", choices=["f16", "bf16", "f32"])
+    ap.add_argument("--err-cols", type=int, default=48)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-plain", action="store_true", help="skip the plain FP32 comparison")
+    ap.add_argument("--skip-error", action="store_true", help="skip the FP64 error check")
+    ap.add_argument("--prefold", action="store_true",
+                    help="fold sqrt(t) into the packed samples (faster, less accurate)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_reference_rate(sv, seconds: float, threads: int):
+    """The reference's psktmCPU.c (oracle/_ref, compiled unmodified) or, where it
+    was never built, the oracle's single-thread restatement, on a bounded sample
+    of the workload: the full image against the first T traces, T sized so the
+    run takes about ``seconds``.  Returns (pairs/s, cores, kind, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    if kind == "port":
+        threads = 1
+    nx, ny, nz = sv.shape
+
+    def run(ntr):
+        tr = np.random.default_rng(5).standard_normal((ntr, sv.nt)).astype(np.float32)
+        args = (sv.imageX, sv.imageY, sv.imageZ, sv.dt, sv.midX[:ntr], sv.midY[:ntr],
+                sv.offX[:ntr], sv.offY[:ntr], tr, sv.velocity1d)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle.migrate_reference_c(*args, threads=threads)
+        else:
+            oracle.migrate_ref32(*args)
+        return time.perf_counter() - t0
+
+    g = oracle.grid
+    sv.imageX, sv.imageY, sv.imageZ = (g(a.imagePnts, a.imageStep, a.imageStart)
+                                       for a in (sv.imageX, sv.imageY, sv.imageZ))
+    t1 = run(1)
+    ntr = int(max(1, min(sv.ntr, seconds / max(t1, 1e-3))))
+    dt = run(ntr)
+    pairs = nx * ny * nz * ntr
+    sample = (f"full {nx}x{ny}x{nz} image x first {ntr} traces ({pairs:.3e} pairs), "
+              f"1-D RMS velocity, {threads} OpenMP threads" if kind == "reference" else
+              f"full image x first {ntr} traces, single-thread oracle restatement")
+    return pairs / dt, threads, kind, sample
+
+
+def reference_arm(a):
+    """--impl reference: the reference's CPU implementation of the path, rank 0."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ktm import synth
+    sv = synth.config2(ntr=20000)
+    threads = os.cpu_count() or 1
+    rates = []
+    budget = max(2.0, 150.0 / max(1, a.steps + a.warmup))
+    info = None
+    for i in range(a.warmup + a.steps):
+        r, cores, kind, sample = cpu_reference_rate(sv, budget, threads)
+        if i >= a.warmup:
+            rates.append(r)
+        info = (cores, kind, sample)
+    v = float(np.mean(rates)) / 1e9
+    cores, kind, sample = info
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "per_step": "bounded CPU sample, see cpu_baseline"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+        return
+    import torch
+
+    import ktm
+    from ktm import synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    # ---- workload: each rank images its own 5 x 5 km tile (weak scaling, no data-path
+    # collective); rank r's survey is the same recipe with seed 2 + r
+    t_setup = time.perf_counter()
+    sv = synth.config2(ntr=a.ntr, seed=2 + rank)
+    T = lambda x: torch.as_tensor(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    vel = T(sv.velocity)
+    vel1 = T(sv.velocity1d)
+    raw = torch.empty((sv.ntr, sv.nt), device=dev, dtype=torch.float32)
+    chunk = 100_000
+    for k0 in range(0, sv.ntr, chunk):
+        synth.synthesize_device(sv, k0, min(sv.ntr, k0 + chunk), device=dev, coords=coords,
+                                out=raw[k0:min(sv.ntr, k0 + chunk)])
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+
+    nb = a.batches
+    bsz = (sv.ntr + nb - 1) // nb
+    bounds = [(b * bsz, min(sv.ntr, (b + 1) * bsz)) for b in range(nb)]
+    nx, ny, nz = sv.shape
+    npts = nx * ny * nz
+    stream = torch.cuda.Stream(device=dev)
+    image = torch.zeros(sv.shape, device=dev, dtype=torch.float32)
+    pitch = ktm.packed_pitch(sv.nt, a.fmt)
+    tdtype = {"f16": torch.float16, "bf16": torch.bfloat16, "f32": torch.float32}[a.fmt]
+    pbuf = torch.empty((bsz, pitch), device=dev, dtype=tdtype)
+    pscale = torch.empty(bsz, device=dev, dtype=torch.float32)
+    counter = torch.zeros(1, device=dev, dtype=torch.int64)
+
+    def step(i, count=False):
+        k0, k1 = bounds[i % nb]
+        n = k1 - k0
+        with torch.cuda.stream(stream):
+            p = ktm.prepare(raw[k0:k1], sv.dt, fmt=a.fmt, rho=sv.rho_opt, prefold=a.prefold,
+                            stream=stream, out=pbuf[:n], out_scale=pscale[:n])
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ktm.migrate(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+                        midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
+                        offY=coords[3][k0:k1], traces=p, velocity=vel, image=image,
+                        pick="linear", aperture=sv.aperture, accumulate=(i > 0), stream=stream,
+                        pairs_counter=counter if count else None)
+            e1.record(stream)
+        return e0, e1, n
+
+    # ---- peaks of this GPU (special-function unit and FP32 FMA pipe)
+    sq, rs, fm = C.c_double(), C.c_double(), C.c_double()
+    ktm._lib.check(ktm.lib().ktmProbePeaks(C.byref(sq), C.byref(rs), C.byref(fm)))
+
+    # ---- warm-up, then K timed steps (events on the launching stream)
+    for i in range(a.warmup):
+        step(i)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    counter.zero_()
+    ev0.record(stream)
+    kev, traces_done = [], 0
+    for i in range(a.steps):
+        # the counter costs one atomic add per warp at kernel exit
+        e0, e1, n = step(i, count=True)
+        kev.append((e0, e1))
+        traces_done += n
+    ev1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    kernel_ms = sum(e0.elapsed_time(e1) for e0, e1 in kev)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    pairs_rank = npts * traces_done
+    value = pairs_rank * world / (ms * 1e-3) / 1e9
+
+    # evaluated pairs (after aperture / end-of-trace culling), counted by the kernel
+    evaluated = int(counter.item())
+    sfu_rate = evaluated * 2 / (kernel_ms * 1e-3)      # two sqrt.approx per evaluated pair
+
+    # ---- accuracy: one batch, fresh image, vs FP64 device evaluation (rho-filtered
+    # FP32 input, weight |tau| sqrt(t) per pair) on sampled columns
+    rel_l2 = max_err = None
+    ncols_err = 0
+    if not a.skip_error:
+        k0, k1 = bounds[0]
+        image_keep = image.clone()
+        image.zero_()
+        step(0)
+        stream.synchronize()
+        p32 = ktm.prepare(raw[k0:k1], sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
+        rng = np.random.default_rng(17)
+        cols = torch.as_tensor(rng.choice(nx * ny, size=min(a.err_cols, nx * ny), replace=False)
+                               .astype(np.int32))
+        ncols_err = len(cols)
+        ref = ktm.migrate_columns_f64(
+            columns=cols, imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+            midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
+            offY=coords[3][k0:k1], traces=p32, velocity=vel, pick="linear", aperture=sv.aperture)
+        # p32 is not prefolded: the FP64 evaluation applies |tau| sqrt(t) per pair
+        got = image.reshape(nx * ny, nz)[cols.to(dev).long()].double()
+        ref = ref.double()
+        rel_l2 = float((got - ref).norm() / ref.norm())
+        max_err = float((got - ref).abs().max() / ref.abs().max())
+        del p32
+        image.copy_(image_keep)
+
+    # ---- plain FP32 path (psktmCPU.c arithmetic, bit-exact kernel) on part of a batch
+    kp = max(1, bsz // 4) if not a.skip_plain else 64
+    plain_kw = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+                    midX=coords[0][:kp], midY=coords[1][:kp], offX=coords[2][:kp],
+                    offY=coords[3][:kp], traces=raw[:kp], velocity=vel1, mode="reference",
+                    pick="truncate", stream=stream)
+    small = dict(plain_kw, midX=coords[0][:64], midY=coords[1][:64], offX=coords[2][:64],
+                 offY=coords[3][:64], traces=raw[:64])
+    pimg = torch.empty(sv.shape, device=dev, dtype=torch.float32)
+    ktm.migrate(image=pimg, **small)
+    stream.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    ktm.migrate(image=pimg, **plain_kw)
+    pe1.record(stream)
+    stream.synchronize()
+    plain_ms = pe0.elapsed_time(pe1)
+    plain_rate = npts * kp / (plain_ms * 1e-3) / 1e9
+    del pimg
+
+    # ---- end to end through the C ABI with host buffers (pinned), per batch:
+    # traces, coordinates, velocity cube host->device, image device->host
+    e2e = None
+    if a.e2e_steps > 0:
+        k0, k1 = bounds[0]
+        n = k1 - k0
+        h_tr = torch.empty((n, sv.nt), dtype=torch.float32, pin_memory=True)
+        h_tr.copy_(raw[k0:k1])
+        h_c = [torch.empty(n, dtype=torch.float32, pin_memory=True).copy_(c[k0:k1]) for c in coords]
+        h_v = torch.empty(vel.shape, dtype=torch.float32, pin_memory=True).copy_(vel)
+        h_img = torch.empty(sv.shape, dtype=torch.float32, pin_memory=True)
+        hk = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+                  midX=h_c[0].numpy(), midY=h_c[1].numpy(), offX=h_c[2].numpy(),
+                  offY=h_c[3].numpy(), traces=h_tr.numpy(), velocity=h_v.numpy(),
+                  image=h_img.numpy(), pick="linear", aperture=sv.aperture, rho=sv.rho_opt,
+                  pack_format=a.fmt, stream=stream)
+        ktm.migrate(**hk)   # warm-up
+        he0, he1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        he0.record(stream)
+        for _ in range(a.e2e_steps):
+            ktm.migrate(**hk)
+        he1.record(stream)
+        stream.synchronize()
+        wall = time.perf_counter() - t0
+        e_ms = max(he0.elapsed_time(he1), wall * 1e3) / a.e2e_steps
+        h2d = n * sv.nt * 4 + 4 * n * 4 + vel.numel() * 4
+        e2e = {"value": npts * n / (e_ms * 1e-3) / 1e9 * world, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 4),
+               "steps": a.e2e_steps, "per_step": "one batch through ktmMigrate, host memory"}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sub = synth.config2(ntr=4096, seed=2)
+        r, cores, kind, sample = cpu_reference_rate(sub, a.cpu_seconds, os.cpu_count() or 1)
+        cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "migrate_fast_traffic.txt")
+    if os.path.exists(tf):
+        for line in open(tf):
+            if line.startswith("dram_bytes_per_trace_per_column:"):
+                per = float(line.split(":")[1])
+                traffic = per * (npts / nz) * bsz
+
+    if rank == 0:
+        per_launch_ms = kernel_ms / a.steps
+        achieved = sfu_rate / 1e12
+        peak = sq.value / 1e12
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": f"{a.fmt} traces, f32 accumulate",
+            "data": "synthetic (seeded, device-generated)",
+            "config": {"workload": WORKLOAD, "traces": sv.ntr, "image": [nx, ny, nz],
+                       "batch_traces": bsz, "trace_format": a.fmt, "rho": "3D (i*omega)",
+                       "pick": "linear", "aperture_m": sv.aperture,
+                       "weight": ("sqrt(j dt) folded into the samples" if a.prefold else
+                                  "sqrt(t) from the interpolated sqrt(j dt) table"),
+                       "l2": "each step reads a new 375 MB batch (> 126 MB L2)",
+                       "parallelism": f"{world} GPU(s), one image tile per GPU, no collective"},
+            "plain_fp32": {"value": plain_rate, "unit": UNIT,
+                           "kernel": "bit-exact psktmCPU.c arithmetic",
+                           "sample": f"{kp} traces x full image, 1-D velocity",
+                           "mixed_over_plain": value / world / plain_rate},
+            "error": {"rel_l2": rel_l2, "max_rel": max_err, "vs": "FP64 device evaluation",
+                      "sample": f"{ncols_err} random image columns x {nz} tau, batch 0"},
+            "pairs": {"raw_per_step": npts * bsz, "evaluated_fraction": evaluated / max(1, pairs_rank),
+                      "evaluated_rate_gpair_s": evaluated / (kernel_ms * 1e-3) / 1e9},
+            "roofline": {"bound": "sfu", "achieved": achieved, "peak": peak, "unit": "Tsqrt/s",
+                         "frac": achieved / peak,
+                         "traffic": traffic,
+                         "note": "2 sqrt.approx per evaluated pair over the migrate kernel's "
+                                 "event time; peak = sqrt.approx throughput measured now "
+                                 "(ktmProbePeaks)",
+                         "kernel_ms_per_launch": per_launch_ms},
+            "peaks_measured": {"sqrt_t_s": sq.value / 1e12, "rsqrt_t_s": rs.value / 1e12,
+                               "ffma_t_s": fm.value / 1e12},
+            "clocks": clk,
+            "e2e": e2e,
+            "gpu_launches": 2 * a.steps,
+            "cpu_baseline": cpu,
+            "setup_s": setup_s,
+        }
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -149,6 +149,9 @@ typedef struct ktm_job {
     int   tileCols;                            /* image columns per CTA (0: tuned) */
     unsigned long long* pairsEvaluated;        /* optional device counter: pairs the
                                                   kernel evaluated (after culling) */
+    /* FAST mode with raw (not packed) traces: the library prepares them first */
+    int   rho;                                 /* KTM_RHO_* pre-filter (ktmApplyRhoFilter.m) */
+    int   packFormat;                          /* KTM_FMT_* of the packed samples */
 } ktm_job;
 
 /* Zero-initialise a job and fill in defaults (mode FAST, pick LINEAR, F32,
@@ -213,6 +216,33 @@ int ktmPrepareTraces(const ktm_prep* prep);
  * measure the error of the FP32 / FP16 / BF16 paths on images too large for a
  * CPU evaluation.  No counterpart in the reference. */
 int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, double* out);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic data and measurement                                           */
+/* ------------------------------------------------------------------------ */
+
+/* Seeded synthetic traces on the device: out[k][j] = sum over scatterers s of
+ * amp_s * Ricker(j*dt - t_ks) + noise * N(0,1), t_ks the double-square-root
+ * time source -> scatterer -> receiver with the scatterer's RMS velocity.
+ * scatterers = double[scatterNo][5] (x, y, tau0, v, amplitude).  The noise is
+ * a counter hash of (seed, traceOffset + k, j), identical to the numpy
+ * generator of the Python package.  All pointers device memory; asynchronous.
+ * Stands in for field data (the reference's impulse option,
+ * ktmWriteTraceBlockConstOffset.m:65-83, is the closest counterpart). */
+int ktmSynthesizeTraces(int traceNo, int tracePts, float sampleRate, const float* midX,
+                        const float* midY, const float* offX, const float* offY,
+                        int scatterNo, const double* scatterers, double freq, double noise,
+                        unsigned long long seed, int traceOffset, float* out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Measurement                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Pipe throughput of the current GPU, measured now: sqrt.approx.f32 and
+ * rsqrt.approx.f32 results per second (the special-function unit that bounds
+ * the migration kernel) and FP32 FMAs per second.  Any pointer may be NULL.
+ * Synchronous.  No counterpart in the reference. */
+int ktmProbePeaks(double* sqrtPerSec, double* rsqrtPerSec, double* ffmaPerSec);
 
 #ifdef __cplusplus
 }

@@ -140,10 +140,16 @@ static int pair_eval(const oracle_job* job, int k, double x, double y, double ta
     g->u = g->t / job->sampleRate;
     /* psktmCPU.c:85: w = t * sqrt(tau^2 / t)  (= |tau| sqrt(t)); with a per-sample
      * weight only the |tau| factor stays per pair */
-    if (job->prefold)
+    if (job->prefold == 3) {
+        /* sqrt(t) by linear interpolation of sqrt(j*dt) between the samples around t */
+        double fl = floor(g->u), f = g->u - fl;
+        double dt = job->sampleRate;
+        g->w = fabs(tau) * ((1.0 - f) * sqrt(fl * dt) + f * sqrt((fl + 1.0) * dt));
+    } else if (job->prefold) {
         g->w = fabs(tau);
-    else
+    } else {
         g->w = (g->t > 0.0) ? g->t * sqrt(tau2 / g->t) : 0.0;
+    }
     return 1;
 }
 

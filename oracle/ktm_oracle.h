@@ -50,7 +50,9 @@ typedef struct oracle_job {
     int prefold;                    /* 0: weight |tau| sqrt(t) per pair (psktmCPU.c:85);
                                        1: |tau| per pair and sqrt(j*dt) per trace sample,
                                           then interpolated; 2: as 1 but the samples
-                                          given already carry sqrt(j*dt) */
+                                          given already carry sqrt(j*dt);
+                                       3: |tau| times sqrt(j*dt) interpolated linearly
+                                          at t/dt (the fast kernel's weight table) */
 } oracle_job;
 
 /* image[p] = sum_k w(p,k) * pick(trace_k, t(p,k)/dt); image overwritten.

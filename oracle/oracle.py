@@ -153,8 +153,9 @@ class _Job:
             self.keep.append(scale)
         ntr, nt = traces.shape
         cube = vel.ndim == 3
+        # the library takes the sample interval as a float (jobParams.traceSampleRate)
         self.job = OracleJob(
-            gx, gy, gz, ntr, nt, nt, float(dt),
+            gx, gy, gz, ntr, nt, nt, float(np.float32(dt)),
             _p(midx), _p(midy), _p(offx), _p(offy), _p(traces),
             _p(scale) if scale is not None else None,
             _p(vel), int(cube), int(pick), float(aperture), int(prefold))

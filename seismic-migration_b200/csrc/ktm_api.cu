@@ -111,16 +111,17 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         a.pick = j->pick; a.aperture = j->aperture;
         a.tileRun = j->tileRun; a.tileCols = j->tileCols;
         a.pairsEvaluated = j->pairsEvaluated;
-        const int wantPrefold = j->pick == KTM_PICK_LINEAR ? 1 : 0;
+        // weight sqrt(t): from the kernel's table (0) or folded into the packed samples (2)
+        a.weightMode = (j->tracesPacked && j->tracesPrefolded) ? 2 : 0;
+        const int wantPrefold = 0;
         if (j->tracesPacked) {
-            if (j->tracesPrefolded != wantPrefold)
-                return set_error(KTM_ERR_ARG, "packed traces: linear pick needs prefold = 1, "
-                                              "truncating pick prefold = 0");
             a.traces = traces; a.scale = scale; a.fmt = j->traceFormat; a.pitch = g.stride;
             if (!scale) return set_error(KTM_ERR_ARG, "packed traces need traceScale");
             return launch_fast(a, s);
         }
-        // raw traces: pack into a temporary F32 set (rho off)
+        // raw traces: filter and pack into a temporary set (job->rho, job->packFormat)
+        if (j->packFormat < KTM_FMT_F32 || j->packFormat > KTM_FMT_BF16)
+            return set_error(KTM_ERR_ARG, "bad packFormat %d", j->packFormat);
         const float* in = static_cast<const float*>(traces);
         void* packed = nullptr;
         float* pscale = nullptr;
@@ -133,8 +134,9 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
             if (rc) return rc;
             src32 = static_cast<const float*>(widened);
         }
-        const int pitch = packed_pitch(g.nt, KTM_FMT_F32);
-        cudaError_t e = cudaMallocAsync(&packed, (size_t)g.ntr * pitch * sizeof(float), s);
+        const int pitch = packed_pitch(g.nt, j->packFormat);
+        const size_t esize = j->packFormat == KTM_FMT_F32 ? 4 : 2;
+        cudaError_t e = cudaMallocAsync(&packed, (size_t)g.ntr * pitch * esize, s);
         if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&pscale), (size_t)g.ntr * 4, s);
         if (e != cudaSuccess) {
             rc = set_error(KTM_ERR_NOMEM, "fast path: packing buffer: %s", cudaGetErrorString(e));
@@ -143,12 +145,12 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
             std::memset(&p, 0, sizeof(p));
             p.traceNo = g.ntr; p.tracePts = g.nt;
             p.inStride = widened ? g.nt : g.stride;
-            p.sampleRate = g.dt; p.in = src32; p.prefold = wantPrefold;
-            p.outFormat = KTM_FMT_F32; p.outPitch = pitch; p.out = packed; p.outScale = pscale;
+            p.sampleRate = g.dt; p.in = src32; p.prefold = wantPrefold; p.rho = j->rho;
+            p.outFormat = j->packFormat; p.outPitch = pitch; p.out = packed; p.outScale = pscale;
             p.stream = s;
             rc = prepare_traces(&p);
             if (!rc) {
-                a.traces = packed; a.scale = pscale; a.fmt = KTM_FMT_F32; a.pitch = pitch;
+                a.traces = packed; a.scale = pscale; a.fmt = j->packFormat; a.pitch = pitch;
                 rc = launch_fast(a, s);
             }
         }

@@ -138,20 +138,28 @@ struct ColInfo {
 
 struct ChunkSmem {
     // layout of one CTA's dynamic shared memory
-    size_t rawBytes, crdOff, geoOff, total;
+    size_t rawBytes, crdOff, geoOff, wtabOff, total;
 };
 
-__host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize)
+__host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize, int nt)
 {
     ChunkSmem L;
     L.rawBytes = (size_t)chunk * pitch * esize;              // one buffer
     L.crdOff = 2 * L.rawBytes;                               // [2][5][chunk] floats
     L.geoOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
-    L.total = L.geoOff + (size_t)chunk * kWarps * sizeof(float4);
+    L.wtabOff = L.geoOff + (size_t)chunk * kWarps * sizeof(float4);
+    L.total = L.wtabOff + (size_t)(nt + 1) * sizeof(float2);   // [nt+1] weight table
     return L;
 }
 
-template <int R, int PICK, int FMT>
+// PRE = 0: weight sqrt(t) from the table (sqrt(j dt), its forward difference)
+//          interpolated with the pair's own fraction f -- relative error
+//          about 1/(32 j^2), far below FP32 interpolation noise for j > 10;
+// PRE = 1: samples prefolded with sqrt(j dt) by ktmPrepareTraces -- one
+//          multiply less per pair, but the interpolation of the product
+//          differs from the reference weight by f(1-f) dg dd (about 6e-4
+//          relative L2 on band-limited data), so it is opt-in.
+template <int R, int PICK, int FMT, int PRE>
 __global__ void __launch_bounds__(kThreads, 2)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
@@ -159,10 +167,11 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
     using T = typename Elem<FMT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Geometry& g = a.g;
-    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T));
+    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt);
     T* rawBase = reinterpret_cast<T*>(smem_raw);
     float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
     float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
+    float2* wtab = reinterpret_cast<float2*>(smem_raw + L.wtabOff);
     __shared__ ColInfo cinfo[kWarps];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -207,6 +216,12 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
         cinfo[warp].y = g.y0 + (float)cj * g.dy;
         cinfo[warp].t2min = t2min;
         cinfo[warp].smin = colValid ? smin : -1.0f;
+    }
+    if (!PRE) {
+        for (int j = threadIdx.x; j <= g.nt; j += kThreads) {
+            const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
+            wtab[j] = make_float2(w0, w1 - w0);
+        }
     }
 
     const int kb = blockIdx.z * perSlice;
@@ -296,16 +311,21 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                     const int i0 = __float_as_int(fl0) - kMagicBits;
                     const int i1 = __float_as_int(fl1) - kMagicBits;
                     const float a0 = Elem<FMT>::get(row, i0), a1 = Elem<FMT>::get(row, i1);
+                    const f2 F = sub2(U, sub2(FL, M2));
+                    f2 V;
                     if (PICK == KTM_PICK_LINEAR) {
                         const float b0 = Elem<FMT>::get(row, i0 + 1), b1 = Elem<FMT>::get(row, i1 + 1);
-                        const f2 F = sub2(U, sub2(FL, M2));
                         const f2 A = pk(a0, a1);
-                        const f2 V = fma2(F, sub2(pk(b0, b1), A), A);
+                        V = fma2(F, sub2(pk(b0, b1), A), A);
+                    } else {
+                        V = pk(a0, a1);
+                    }
+                    if (PRE) {
                         acc[h] = fma2(SC, V, acc[h]);
                     } else {
-                        // weight sqrt(t) per pair (u in samples; sqrt(dt) applied at the end)
-                        const f2 W = mul2(SC, pk(sqrt_approx(u0), sqrt_approx(u1)));
-                        acc[h] = fma2(W, pk(a0, a1), acc[h]);
+                        const float2 w0 = wtab[i0], w1 = wtab[i1];
+                        const f2 W = fma2(F, pk(w0.y, w1.y), pk(w0.x, w1.x));
+                        acc[h] = fma2(mul2(SC, W), V, acc[h]);
                     }
                 }
             }
@@ -313,7 +333,6 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
     }
 
     if (colValid) {
-        const float wscale = PICK == KTM_PICK_LINEAR ? 1.0f : sqrtf(g.dt);
         const size_t nimg = (size_t)ncols * g.nz;
         float* out = partial ? partial + blockIdx.z * nimg + (size_t)col * g.nz
                              : a.image + (size_t)col * g.nz;
@@ -326,7 +345,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                 const int l = run0 + lane + 32 * (2 * h + e);
                 if (l < g.nz) {
                     const float tau = fabsf(g.z0 + (float)l * g.dz);
-                    const float v = v2[e] * (tau * wscale);
+                    const float v = v2[e] * tau;
                     out[l] = (!partial && a.accumulate) ? out[l] + v : v;
                 }
             }
@@ -347,18 +366,18 @@ __global__ void reduce_slices(float* __restrict__ out, const float* __restrict__
     }
 }
 
-template <int R, int PICK, int FMT>
+template <int R, int PICK, int FMT, int PRE>
 int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const Geometry& g = a.g;
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
     int chunk = 32;
-    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize).total > kFastSmemBudget) chunk--;
-    if (chunk_layout(chunk, a.pitch, esize).total > (size_t)kMaxSmemBytes)
+    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize, g.nt).total > kFastSmemBudget) chunk--;
+    if (chunk_layout(chunk, a.pitch, esize, g.nt).total > (size_t)kMaxSmemBytes)
         return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
                                         "stage limit", a.pitch);
-    const size_t smem = chunk_layout(chunk, a.pitch, esize).total;
-    auto kern = fast_kernel<R, PICK, FMT>;
+    const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt).total;
+    auto kern = fast_kernel<R, PICK, FMT, PRE>;
     KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     const long long cols = (long long)g.nx * g.ny;
@@ -401,21 +420,25 @@ int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
     return KTM_OK;
 }
 
-template <int R, int PICK>
+template <int R, int PICK, int PRE>
 int launch_fmt(const FastArgs& a, cudaStream_t s, int sm)
 {
     switch (a.fmt) {
-        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32>(a, s, sm);
-        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16>(a, s, sm);
-        default: return launch_t<R, PICK, KTM_FMT_BF16>(a, s, sm);
+        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32, PRE>(a, s, sm);
+        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16, PRE>(a, s, sm);
+        default: return launch_t<R, PICK, KTM_FMT_BF16, PRE>(a, s, sm);
     }
 }
 
 template <int R>
 int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
 {
-    return a.pick == KTM_PICK_LINEAR ? launch_fmt<R, KTM_PICK_LINEAR>(a, s, sm)
-                                     : launch_fmt<R, KTM_PICK_TRUNCATE>(a, s, sm);
+    if (a.pick == KTM_PICK_LINEAR)
+        return a.weightMode == 2 ? launch_fmt<R, KTM_PICK_LINEAR, 1>(a, s, sm)
+                                 : launch_fmt<R, KTM_PICK_LINEAR, 0>(a, s, sm);
+    if (a.weightMode == 2)
+        return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
+    return launch_fmt<R, KTM_PICK_TRUNCATE, 0>(a, s, sm);
 }
 
 // ---------------------------------------------------------------------------

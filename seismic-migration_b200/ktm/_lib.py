@@ -68,6 +68,7 @@ class KtmJob(C.Structure):
         ("stream", P),
         ("tileRun", C.c_int), ("tileCols", C.c_int),
         ("pairsEvaluated", P),
+        ("rho", C.c_int), ("packFormat", C.c_int),
     ]
 
 
@@ -117,6 +118,11 @@ def lib() -> C.CDLL:
     L.ktmPackedPitch.restype = C.c_int
     L.ktmPrepareTraces.argtypes = [C.POINTER(KtmPrep)]
     L.ktmPrepareTraces.restype = C.c_int
+    L.ktmProbePeaks.argtypes = [P, P, P]
+    L.ktmProbePeaks.restype = C.c_int
+    L.ktmSynthesizeTraces.argtypes = [C.c_int, C.c_int, C.c_float, P, P, P, P, C.c_int, P,
+                                      C.c_double, C.c_double, C.c_ulonglong, C.c_int, P, P]
+    L.ktmSynthesizeTraces.restype = C.c_int
     _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "

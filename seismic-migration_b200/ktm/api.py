@@ -178,7 +178,7 @@ class Job:
     def __init__(self, *, imageX, imageY, imageZ, dt, midX, midY, offX, offY, traces,
                  velocity, image=None, scale=None, mode="fast", pick="linear",
                  aperture=0.0, accumulate=False, prefolded=False, fmt=None, stream=None,
-                 tile_run=0, pairs_counter=None, trace_stride=0):
+                 tile_run=0, pairs_counter=None, trace_stride=0, rho=0, pack_format="f32"):
         packed = None
         if isinstance(traces, PackedTraces):
             packed = traces
@@ -240,6 +240,8 @@ class Job:
         j.stream = _stream_handle(stream)
         j.tileRun = int(tile_run)
         j.pairsEvaluated = _ptr(pairs_counter)
+        j.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
+        j.packFormat = _FMT[pack_format]
         self.job = j
 
     def run(self):
@@ -260,10 +262,10 @@ def migrate_columns_f64(*, columns=None, ncols=None, **kw):
         raise ValueError("migrate_columns_f64 takes CUDA tensors")
     nz = kw["imageZ"].imagePnts
     if columns is not None:
-        cols = columns.to(device=kw["traces"].device, dtype=torch.int32).contiguous()
+        cols = columns.to(device=kw["midX"].device, dtype=torch.int32).contiguous()
         n = cols.numel()
     else:
         cols, n = None, int(ncols)
-    out = torch.empty((n, nz), device=kw["traces"].device, dtype=torch.float64)
+    out = torch.empty((n, nz), device=kw["midX"].device, dtype=torch.float64)
     check(lib().ktmMigrateColumnsF64(C.byref(job.job), _ptr(cols), int(n), out.data_ptr()))
     return out

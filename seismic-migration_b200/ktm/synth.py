@@ -204,6 +204,35 @@ def config4(seed=4) -> Survey:
 
 
 # ---------------------------------------------------------------------------- traces ---
+def synthesize_device(sv: Survey, k0: int = 0, k1: int | None = None, device="cuda",
+                      coords=None, out=None, stream=None):
+    """Device traces [k1-k0, nt] float32 from ktmSynthesizeTraces (same recipe
+    and noise as ``synthesize``).  ``coords`` = (midX, midY, offX, offY) CUDA
+    tensors of the whole survey, to avoid re-uploading them."""
+    import ctypes as C
+
+    import torch
+
+    from ._lib import check, lib
+    k1 = sv.ntr if k1 is None else k1
+    n = k1 - k0
+    if coords is None:
+        coords = [torch.as_tensor(np.ascontiguousarray(a)).to(device)
+                  for a in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    scat = torch.as_tensor(np.ascontiguousarray(sv.scat, dtype=np.float64)).to(device)
+    if out is None:
+        out = torch.empty((n, sv.nt), device=device, dtype=torch.float32)
+    mx, my, ox, oy = (c[k0:k1] for c in coords)
+    stream_h = None if stream is None else stream.cuda_stream
+    check(lib().ktmSynthesizeTraces(
+        int(n), int(sv.nt), float(sv.dt), mx.data_ptr(), my.data_ptr(), ox.data_ptr(),
+        oy.data_ptr(), int(scat.shape[0]), scat.data_ptr(), float(sv.freq), float(sv.noise),
+        C.c_ulonglong(int(sv.seed)), int(sv.meta.get("trace_offset", 0) + k0), out.data_ptr(),
+        stream_h))
+    torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+    return out
+
+
 def synthesize(sv: Survey, k0: int = 0, k1: int | None = None, noise: bool = True) -> np.ndarray:
     """Numpy traces [k1-k0, nt] float32 (CPU; meant for small surveys)."""
     k1 = sv.ntr if k1 is None else k1
