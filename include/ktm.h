@@ -152,7 +152,17 @@ typedef struct ktm_job {
     /* FAST mode with raw (not packed) traces: the library prepares them first */
     int   rho;                                 /* KTM_RHO_* pre-filter (ktmApplyRhoFilter.m) */
     int   packFormat;                          /* KTM_FMT_* of the packed samples */
+    int   weightMethod;                        /* KTM_WEIGHT_*: how FAST mode evaluates the
+                                                  sqrt(t) of the weight when the samples
+                                                  do not carry it */
 } ktm_job;
+
+/* sqrt(t) of the reference weight t*sqrt(tau^2/t) = |tau| sqrt(t) (psktmCPU.c:85). */
+enum {
+    KTM_WEIGHT_TABLE = 0,   /* sqrt(j*dt) table interpolated at t/dt (relative error
+                               ~1/(32 j^2)) -- two special-function ops per pair */
+    KTM_WEIGHT_SQRT = 1     /* sqrt.approx per pair -- three special-function ops */
+};
 
 /* Zero-initialise a job and fill in defaults (mode FAST, pick LINEAR, F32,
  * overwrite, host memory, tuned tiles). */

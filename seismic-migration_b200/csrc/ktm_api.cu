@@ -113,6 +113,9 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         a.pairsEvaluated = j->pairsEvaluated;
         // weight sqrt(t): from the kernel's table (0) or folded into the packed samples (2)
         a.weightMode = (j->tracesPacked && j->tracesPrefolded) ? 2 : 0;
+        if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
+            return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
+        a.weightMethod = j->weightMethod;
         const int wantPrefold = 0;
         if (j->tracesPacked) {
             a.traces = traces; a.scale = scale; a.fmt = j->traceFormat; a.pitch = g.stride;

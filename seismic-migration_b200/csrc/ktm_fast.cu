@@ -117,6 +117,65 @@ template <> struct Elem<KTM_FMT_F16> {
     static __device__ __forceinline__ float get(const T* p, int i) { return __half2float(p[i]); }
 };
 
+// Shared-memory loads through 32-bit shared addresses.  The sample index comes
+// out of the round-down magic add as bits(fl) = 0x4B400000 + i0, so the row
+// base is pre-offset by -0x4B400000 * sizeof(T) (mod 2^32) and the address is
+// one multiply-add of the float's bits.  Volatile: these loads must stay
+// between the barriers that bracket each chunk.
+template <int FMT> struct Lds;
+template <> struct Lds<KTM_FMT_F32> {
+    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
+    {
+        asm volatile("ld.shared.f32 %0, [%2];\n\tld.shared.f32 %1, [%2+4];" : "=f"(a), "=f"(b) : "r"(ad));
+    }
+    static __device__ __forceinline__ float one(unsigned ad)
+    {
+        float a;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(a) : "r"(ad));
+        return a;
+    }
+};
+template <> struct Lds<KTM_FMT_BF16> {
+    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
+    {
+        unsigned short x, y;
+        asm volatile("ld.shared.u16 %0, [%2];\n\tld.shared.u16 %1, [%2+2];" : "=h"(x), "=h"(y) : "r"(ad));
+        a = __uint_as_float(static_cast<unsigned>(x) << 16);
+        b = __uint_as_float(static_cast<unsigned>(y) << 16);
+    }
+    static __device__ __forceinline__ float one(unsigned ad)
+    {
+        unsigned short x;
+        asm volatile("ld.shared.u16 %0, [%1];" : "=h"(x) : "r"(ad));
+        return __uint_as_float(static_cast<unsigned>(x) << 16);
+    }
+};
+template <> struct Lds<KTM_FMT_F16> {
+    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
+    {
+        unsigned short x, y;
+        asm volatile("ld.shared.b16 %0, [%2];\n\tld.shared.b16 %1, [%2+2];" : "=h"(x), "=h"(y) : "r"(ad));
+        a = __half2float(__ushort_as_half(x));
+        b = __half2float(__ushort_as_half(y));
+    }
+    static __device__ __forceinline__ float one(unsigned ad)
+    {
+        unsigned short x;
+        asm volatile("ld.shared.b16 %0, [%1];" : "=h"(x) : "r"(ad));
+        return __half2float(__ushort_as_half(x));
+    }
+};
+__device__ __forceinline__ float2 lds_f2(unsigned ad)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(ad));
+    return v;
+}
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -152,13 +211,17 @@ __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch,
     return L;
 }
 
-// PRE = 0: weight sqrt(t) from the table (sqrt(j dt), its forward difference)
-//          interpolated with the pair's own fraction f -- relative error
-//          about 1/(32 j^2), far below FP32 interpolation noise for j > 10;
-// PRE = 1: samples prefolded with sqrt(j dt) by ktmPrepareTraces -- one
-//          multiply less per pair, but the interpolation of the product
-//          differs from the reference weight by f(1-f) dg dd (about 6e-4
-//          relative L2 on band-limited data), so it is opt-in.
+// Weight sqrt(t) of each pair (PRE):
+//   kWtTable   sqrt(j dt) and its forward difference from a per-CTA table,
+//              interpolated with the pair's own fraction f: relative error
+//              about 1/(32 j^2), far below FP32 interpolation noise for j > 10;
+//   kWtPrefold samples prefolded with sqrt(j dt) by ktmPrepareTraces: one
+//              multiply less per pair, but the interpolation of the product
+//              differs from the reference weight by f(1-f) dg dd (about 6e-4
+//              relative L2 on shallow band-limited data), so it is opt-in;
+//   kWtSqrt    a third sqrt.approx per pair on the special-function unit.
+constexpr int kWtTable = 0, kWtPrefold = 1, kWtSqrt = 2;
+
 template <int R, int PICK, int FMT, int PRE>
 __global__ void __launch_bounds__(kThreads, 2)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
@@ -217,7 +280,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
         cinfo[warp].t2min = t2min;
         cinfo[warp].smin = colValid ? smin : -1.0f;
     }
-    if (!PRE) {
+    if (PRE == kWtTable) {
         for (int j = threadIdx.x; j <= g.nt; j += kThreads) {
             const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
             wtab[j] = make_float2(w0, w1 - w0);
@@ -285,13 +348,15 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
         }
         __syncthreads();
         if (colValid) {
-            const T* rows = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(rawBase) +
-                                                       b * L.rawBytes);
+            const unsigned rowsS = smem_u32(reinterpret_cast<const unsigned char*>(rawBase) + b * L.rawBytes);
+            // bits(fl) = kMagicBits + i0: fold the magic offset into the bases (mod 2^32)
+            const unsigned magicT = (unsigned)kMagicBits * (unsigned)sizeof(T);
+            const unsigned wS = smem_u32(wtab) - (unsigned)kMagicBits * 8u;
             for (int c = 0; c < n; c++) {
                 const float4 gd = geo[c * kWarps + warp];
                 if (gd.x < 0.0f) continue;                 // warp-uniform
                 evaluated += nvalid;
-                const T* row = rows + (size_t)c * a.pitch;
+                const unsigned rowS = rowsS + (unsigned)(c * a.pitch) * (unsigned)sizeof(T) - magicT;
                 const f2 DS = pk(gd.x, gd.x), DR = pk(gd.y, gd.y), SC = pk(gd.z, gd.z);
 #pragma unroll
                 for (int h = 0; h < R / 2; h++) {
@@ -308,23 +373,29 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                     const f2 FL = add2_rm(U, M2);
                     float fl0, fl1;
                     upk(FL, fl0, fl1);
-                    const int i0 = __float_as_int(fl0) - kMagicBits;
-                    const int i1 = __float_as_int(fl1) - kMagicBits;
-                    const float a0 = Elem<FMT>::get(row, i0), a1 = Elem<FMT>::get(row, i1);
+                    const unsigned q0 = __float_as_uint(fl0), q1 = __float_as_uint(fl1);
+                    const unsigned ad0 = rowS + q0 * (unsigned)sizeof(T);
+                    const unsigned ad1 = rowS + q1 * (unsigned)sizeof(T);
                     const f2 F = sub2(U, sub2(FL, M2));
                     f2 V;
                     if (PICK == KTM_PICK_LINEAR) {
-                        const float b0 = Elem<FMT>::get(row, i0 + 1), b1 = Elem<FMT>::get(row, i1 + 1);
+                        float a0, b0, a1, b1;
+                        Lds<FMT>::pair(ad0, a0, b0);
+                        Lds<FMT>::pair(ad1, a1, b1);
                         const f2 A = pk(a0, a1);
                         V = fma2(F, sub2(pk(b0, b1), A), A);
                     } else {
-                        V = pk(a0, a1);
+                        V = pk(Lds<FMT>::one(ad0), Lds<FMT>::one(ad1));
                     }
-                    if (PRE) {
+                    if (PRE == kWtPrefold) {
                         acc[h] = fma2(SC, V, acc[h]);
-                    } else {
-                        const float2 w0 = wtab[i0], w1 = wtab[i1];
+                    } else if (PRE == kWtTable) {
+                        const float2 w0 = lds_f2(wS + q0 * 8u), w1 = lds_f2(wS + q1 * 8u);
                         const f2 W = fma2(F, pk(w0.y, w1.y), pk(w0.x, w1.x));
+                        acc[h] = fma2(mul2(SC, W), V, acc[h]);
+                    } else {
+                        // u is in samples: sqrt(t) = sqrt(u) sqrt(dt), sqrt(dt) applied at the end
+                        const f2 W = pk(sqrt_approx(u0), sqrt_approx(u1));
                         acc[h] = fma2(mul2(SC, W), V, acc[h]);
                     }
                 }
@@ -345,7 +416,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                 const int l = run0 + lane + 32 * (2 * h + e);
                 if (l < g.nz) {
                     const float tau = fabsf(g.z0 + (float)l * g.dz);
-                    const float v = v2[e] * tau;
+                    const float v = v2[e] * (PRE == kWtSqrt ? tau * sqrtf(g.dt) : tau);
                     out[l] = (!partial && a.accumulate) ? out[l] + v : v;
                 }
             }
@@ -433,12 +504,18 @@ int launch_fmt(const FastArgs& a, cudaStream_t s, int sm)
 template <int R>
 int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
 {
+    // a.weightMode: 2 samples prefolded; otherwise a.weightMethod picks table / sqrt
+    if (a.weightMode == 2) {
+        if (a.pick != KTM_PICK_LINEAR)
+            return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
+        return launch_fmt<R, KTM_PICK_LINEAR, kWtPrefold>(a, s, sm);
+    }
+    const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
     if (a.pick == KTM_PICK_LINEAR)
-        return a.weightMode == 2 ? launch_fmt<R, KTM_PICK_LINEAR, 1>(a, s, sm)
-                                 : launch_fmt<R, KTM_PICK_LINEAR, 0>(a, s, sm);
-    if (a.weightMode == 2)
-        return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
-    return launch_fmt<R, KTM_PICK_TRUNCATE, 0>(a, s, sm);
+        return sq ? launch_fmt<R, KTM_PICK_LINEAR, kWtSqrt>(a, s, sm)
+                  : launch_fmt<R, KTM_PICK_LINEAR, kWtTable>(a, s, sm);
+    return sq ? launch_fmt<R, KTM_PICK_TRUNCATE, kWtSqrt>(a, s, sm)
+              : launch_fmt<R, KTM_PICK_TRUNCATE, kWtTable>(a, s, sm);
 }
 
 // ---------------------------------------------------------------------------

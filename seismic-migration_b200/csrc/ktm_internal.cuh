@@ -52,6 +52,7 @@ struct FastArgs {
     // FP64 reference only: 0 weight |tau| sqrt(t) per pair; 1 sqrt(j*dt) applied
     // to each sample; 2 samples already carry sqrt(j*dt)
     int weightMode;
+    int weightMethod;       // KTM_WEIGHT_* when the samples do not carry sqrt(j*dt)
     const float* vel; int velCube;
     float* image; int accumulate;
     int pick; float aperture;

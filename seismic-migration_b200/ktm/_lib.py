@@ -68,7 +68,7 @@ class KtmJob(C.Structure):
         ("stream", P),
         ("tileRun", C.c_int), ("tileCols", C.c_int),
         ("pairsEvaluated", P),
-        ("rho", C.c_int), ("packFormat", C.c_int),
+        ("rho", C.c_int), ("packFormat", C.c_int), ("weightMethod", C.c_int),
     ]
 
 

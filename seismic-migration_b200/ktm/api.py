@@ -178,7 +178,8 @@ class Job:
     def __init__(self, *, imageX, imageY, imageZ, dt, midX, midY, offX, offY, traces,
                  velocity, image=None, scale=None, mode="fast", pick="linear",
                  aperture=0.0, accumulate=False, prefolded=False, fmt=None, stream=None,
-                 tile_run=0, pairs_counter=None, trace_stride=0, rho=0, pack_format="f32"):
+                 tile_run=0, pairs_counter=None, trace_stride=0, rho=0, pack_format="f32",
+                 weight="table"):
         packed = None
         if isinstance(traces, PackedTraces):
             packed = traces
@@ -242,6 +243,7 @@ class Job:
         j.pairsEvaluated = _ptr(pairs_counter)
         j.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
         j.packFormat = _FMT[pack_format]
+        j.weightMethod = {"table": 0, "sqrt": 1}[weight]
         self.job = j
 
     def run(self):
