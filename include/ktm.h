@@ -220,6 +220,24 @@ int ktmPackedPitch(int tracePts, int format);
  * pre-processing ktmApplyRhoFilter.m with a device step.  Asynchronous. */
 int ktmPrepareTraces(const ktm_prep* prep);
 
+/* ktmMigrate for callers that cannot allocate device memory while they run:
+ * a processing loop that must never let cudaMalloc / cudaFree synchronise the
+ * device, or a host framework that has already shared the GPU's memory out
+ * among its own pools.  No counterpart in the reference.
+ *   - Takes FAST mode, device memory and a packed trace set (ktmPrepareTraces);
+ *     the caller passes every input and the output image as usual.
+ *   - Calls no cudaMalloc, cudaFree or allocating routine.  Its only scratch,
+ *     the partial images of the trace slices, is a static 16 MiB device array
+ *     (4 Mi floats) that each GPU loading the library keeps until exit.
+ *   - Limit: images of at most 2 Mi samples (Nx*Ny*Nz <= 2097152); larger
+ *     images are rejected with KTM_ERR_LIMIT.
+ *   - The first call on a device looks up that device's copy of the array
+ *     (with the device current); make that first call before any stream capture.
+ *   - Every call uses the same array: calls that overlap on the GPU (other
+ *     streams, other host threads on the same device) race.  Nothing in the
+ *     array has to start at zero; each call overwrites what it reads. */
+int ktmMigratePackedNoAlloc(const ktm_job* job);
+
 /* FP64 device evaluation of the job's method (pick, aperture, Vrms cube,
  * weight) for the image columns columns[0..ncols) (column index = ix*Ny + iy;
  * columns == NULL: 0..ncols-1): out[q][Nz].  Device memory only.  Used to

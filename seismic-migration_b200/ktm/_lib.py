@@ -118,6 +118,8 @@ def lib() -> C.CDLL:
     L.ktmPackedPitch.restype = C.c_int
     L.ktmPrepareTraces.argtypes = [C.POINTER(KtmPrep)]
     L.ktmPrepareTraces.restype = C.c_int
+    L.ktmMigratePackedNoAlloc.argtypes = [C.POINTER(KtmJob)]
+    L.ktmMigratePackedNoAlloc.restype = C.c_int
     L.ktmProbePeaks.argtypes = [P, P, P]
     L.ktmProbePeaks.restype = C.c_int
     L.ktmSynthesizeTraces.argtypes = [C.c_int, C.c_int, C.c_float, P, P, P, P, C.c_int, P,
