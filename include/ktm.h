@@ -220,6 +220,46 @@ int ktmPackedPitch(int tracePts, int format);
  * pre-processing ktmApplyRhoFilter.m with a device step.  Asynchronous. */
 int ktmPrepareTraces(const ktm_prep* prep);
 
+/* ------------------------------------------------------------------------ */
+/* Adjoint, velocity gradient, least-squares migration                      */
+/* (no counterpart in the reference: it has no adjoint and no inversion)    */
+/* ------------------------------------------------------------------------ */
+
+/* Kirchhoff demigration, the exact transpose of ktmMigrate in FAST mode
+ * (linear or truncating pick, KTM_WEIGHT_TABLE or KTM_WEIGHT_SQRT, aperture,
+ * Vrms): reads the model from job->image [Nx][Ny][Nz] and writes
+ *   data[k][j] = sum_p w(p,k) coef_j(t(p,k)/dt) m[p],   0 < j < tracePts,
+ * into the packed F32 layout [traceNo][dataPitch] (dataPitch >= tracePts + 2,
+ * a multiple of 4; zero guard samples), overwritten unless job->accumulate.
+ * job->traces is not read.  Device memory, asynchronous on job->stream. */
+int ktmDemigrate(const ktm_job* job, float* data, int dataPitch);
+
+/* Sensitivity of the migrated image to the RMS velocity at each image sample:
+ * grad[p] = dI[p] / dv[p] for the job's packed traces (linear pick; table
+ * weight or prefolded samples) -- the traveltime (and weight) derivative of
+ * every pair, d/dv of t = sqrt(tau^2 + |s-x|^2/v^2) + sqrt(tau^2 + |r-x|^2/v^2).
+ * For an objective J(I), dJ/dv[p] = dJ/dI[p] * grad[p].  grad is
+ * [Nx][Ny][Nz], device memory; asynchronous. */
+int ktmVrmsGradient(const ktm_job* job, float* grad);
+
+/* Least-squares migration by conjugate gradients on the normal equations
+ * (CGLS): minimise || L m - d ||^2, L = ktmDemigrate, L^T = ktmMigrate (FAST
+ * mode, packed F32 traces).  All vectors and scalars stay on the device; the
+ * CG dot products and norms are FP64.  With useGraph = 1 one iteration is
+ * captured in a CUDA graph and replayed. */
+typedef struct ktm_lsm {
+    ktm_job job;                 /* geometry, coordinates, velocity, pick, aperture,
+                                    weightMethod, stream; device memory */
+    const float* data;           /* observed data, packed F32 [traceNo][dataPitch] */
+    int   dataPitch;
+    float* model;                /* [Nx][Ny][Nz]: starting model in, solution out */
+    int   iterations;
+    int   useGraph;
+    double* residualNorms;       /* host [iterations+1]: ||d - L m_i|| (may be NULL) */
+    double* gradientNorms;       /* host [iterations+1]: ||L^T (d - L m_i)|| (may be NULL) */
+} ktm_lsm;
+int ktmLeastSquaresMigrate(const ktm_lsm* lsm);
+
 /* ktmMigrate for callers that cannot allocate device memory while they run:
  * a processing loop that must never let cudaMalloc / cudaFree synchronise the
  * device, or a host framework that has already shared the GPU's memory out

@@ -247,7 +247,11 @@ void oracle_vrms_grad_f64(const oracle_job* job, double* grad)
                 double val = (1.0 - f) * s0 + f * s1;
                 double dval_du = s1 - s0;
                 double dt_dS = g.ds2 / (2.0 * sqrt(g.as_)) + g.dr2 / (2.0 * sqrt(g.ar_));
-                double dw_dt = job->prefold ? 0.0 : fabs(tau) / (2.0 * sqrt(g.t));
+                double dw_dt;
+                if (job->prefold == 3)      /* table weight: slope of the interpolated sqrt(j dt) */
+                    dw_dt = fabs(tau) * (sqrt((fl + 1.0) * job->sampleRate) - sqrt(fl * job->sampleRate)) / job->sampleRate;
+                else
+                    dw_dt = job->prefold ? 0.0 : fabs(tau) / (2.0 * sqrt(g.t));
                 acc += (dw_dt * val + g.w * dval_du / job->sampleRate) * dt_dS;
             }
             grad[(size_t)c * Nz + l] = acc * (-2.0 / (v * v * v));

@@ -109,6 +109,7 @@ def grid(n: int, step: float, start: float) -> ImageGrid:
 
 
 def _ref_args(gx, gy, gz, ntr, nt, dt, midx, midy, offx, offy, traces, vel, image):
+    gx, gy, gz = _as_grid(gx), _as_grid(gy), _as_grid(gz)
     cfg = JobParams(int(ntr), int(nt), float(dt))
     return [C.byref(gx), C.byref(gy), C.byref(gz), C.byref(cfg),
             _p(midx), _p(midy), _p(offx), _p(offy), _p(traces), _p(vel), _p(image)]
@@ -141,11 +142,19 @@ def migrate_reference_c(gx, gy, gz, dt, midx, midy, offx, offy, traces, vel,
     return image
 
 
+def _as_grid(g) -> ImageGrid:
+    """Any object with imagePnts / imageStep / imageStart (e.g. the product's own grid)."""
+    if isinstance(g, ImageGrid):
+        return g
+    return ImageGrid(int(g.imagePnts), float(g.imageStep), float(g.imageStart))
+
+
 class _Job:
     """Holds an OracleJob and the arrays it points at."""
 
     def __init__(self, gx, gy, gz, dt, midx, midy, offx, offy, traces, vel, *,
                  scale=None, pick=1, aperture=0.0, prefold=False):
+        gx, gy, gz = _as_grid(gx), _as_grid(gy), _as_grid(gz)
         self.keep = [_f32(a) for a in (midx, midy, offx, offy, traces, vel)]
         midx, midy, offx, offy, traces, vel = self.keep
         if scale is not None:

@@ -1,0 +1,274 @@
+// ktm_adjoint.cu -- Kirchhoff demigration: the exact transpose of the fast
+// migration operator (ktm_fast.cu) for its linear and truncating picks and
+// its table / sqrt weights.  The reference has no adjoint; this operator is
+// what least-squares migration (ktm_lsm.cu) and the dot-product test need.
+//
+// Migration (linear pick):  I[p] = |tau_p| sum_k s_k W_pk (q_k[i0] + f (q_k[i0+1] - q_k[i0]))
+// Demigration:              D_k[i0]   += W_pk |tau_p| m[p] (1 - f)
+//                           D_k[i0+1] += W_pk |tau_p| m[p] f          (0 < j < tracePts only)
+// Every pair's (u, f, i0, W) comes from the same code as the migration's
+// (ktm_pair.cuh), so the two operators are transposes pair by pair.
+//
+// Work decomposition: a CTA owns a chunk of traces, accumulates their samples
+// in shared memory (red.shared.add) while its warps sweep the image columns of
+// its column block, and writes the chunk out once (plain stores when one block
+// covers all columns, red.global.add otherwise).  A warp covers one column x a
+// run of 32*R tau samples at a time, as in the migration; the model samples,
+// the tau tables and the velocity of the run stay in registers for all the
+// chunk's traces.
+#include "ktm_pair.cuh"
+
+#include <algorithm>
+
+namespace ktm {
+namespace {
+
+using namespace dev;
+
+constexpr int kAdjWarps = 8;
+constexpr int kAdjThreads = kAdjWarps * 32;
+constexpr int kAdjR = 16;                // tau samples per lane per run
+constexpr size_t kAdjSmemBudget = 100 * 1024;
+
+struct AdjArgs {
+    Geometry g;
+    const float *midX, *midY, *offX, *offY;
+    const float* vel; int velCube;
+    const float* image;      // model m [nx*ny][nz]
+    float* data;             // [ntr][pitch] F32
+    int pitch;
+    int pick, weightMethod;
+    float aperture;
+    int chunk;               // traces per CTA
+    int colsPerBlock;        // image columns per CTA (gridDim.y blocks)
+    int atomicOut;           // 1: red.global.add into data (several column blocks)
+};
+
+// Volatile, so the scatter stays between the barriers around the sweep; no
+// "memory" clobber, so the arithmetic around it still schedules freely.
+__device__ __forceinline__ void red_shared(unsigned addr, float v)
+{
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(addr), "f"(v));
+}
+
+// Scatter-add from the 32 lanes of a warp.  FP32 shared-memory atomics run at
+// ~7 per clock per SM on distinct addresses but serialise on equal ones (0.3
+// per clock at 32 lanes per address, measured on B200) -- and the lanes of a
+// warp hold consecutive tau samples of one trace, so where t(tau) is flat
+// (shallow, far offsets) runs of lanes hit the same sample.  When a warp has
+// such a run, the run is summed into its first lane by a segmented suffix sum
+// (five shuffles) and only that lane issues the atomic.
+__device__ __forceinline__ void scatter_add(unsigned addr, float v, int lane)
+{
+    const unsigned prev = __shfl_up_sync(0xffffffffu, addr, 1);
+    const bool dup = lane > 0 && prev == addr;
+    if (!__any_sync(0xffffffffu, dup)) {
+        red_shared(addr, v);
+        return;
+    }
+    const unsigned heads = __ballot_sync(0xffffffffu, !dup);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_down_sync(0xffffffffu, v, o);
+        // lane + o belongs to this lane's run iff no run starts in (lane, lane + o]
+        if (lane + o < 32 && ((heads >> (lane + 1)) & ((1u << o) - 1u)) == 0u) v += t;
+    }
+    if (!dup) red_shared(addr, v);
+}
+
+template <int PICK, int WT>
+__global__ void __launch_bounds__(kAdjThreads)
+demigrate_kernel(AdjArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Geometry& g = a.g;
+    float* acc = reinterpret_cast<float*>(smem_raw);                    // [chunk][pitch]
+    float* crd = acc + (size_t)a.chunk * a.pitch;                       // [4][chunk]
+    float2* wtab = reinterpret_cast<float2*>(crd + 4 * a.chunk + ((4 * a.chunk) & 1));  // [nt+1]
+
+    const int k0 = blockIdx.x * a.chunk;
+    const int n = min(a.chunk, g.ntr - k0);
+    for (int i = threadIdx.x; i < a.chunk * a.pitch; i += kAdjThreads) acc[i] = 0.0f;
+    for (int i = threadIdx.x; i < n; i += kAdjThreads) {
+        crd[i] = a.midX[k0 + i];
+        crd[a.chunk + i] = a.midY[k0 + i];
+        crd[2 * a.chunk + i] = a.offX[k0 + i];
+        crd[3 * a.chunk + i] = a.offY[k0 + i];
+    }
+    if (WT == 0) {
+        for (int j = threadIdx.x; j <= g.nt; j += kAdjThreads) {
+            const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
+            wtab[j] = make_float2(w0, w1 - w0);
+        }
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ncols = g.nx * g.ny;
+    const int cb0 = blockIdx.y * a.colsPerBlock;
+    const int cb1 = min(ncols, cb0 + a.colsPerBlock);
+    const float invdt = 1.0f / g.dt;
+    const float umax = (float)g.nt;
+    const float ap2 = a.aperture > 0.0f ? a.aperture * a.aperture : -1.0f;
+    const f2 M2 = pk(kMagic, kMagic);
+    const unsigned accS = smem_u32(acc) - (unsigned)kMagicBits * 4u;
+    const unsigned wS = smem_u32(wtab) - (unsigned)kMagicBits * 8u;
+    const int nruns = (g.nz + 32 * kAdjR - 1) / (32 * kAdjR);
+
+    for (int col = cb0 + warp; col < cb1; col += kAdjWarps) {
+        const int ci = col / g.ny, cj = col % g.ny;
+        const float cx = g.x0 + (float)ci * g.dx, cy = g.y0 + (float)cj * g.dy;
+        for (int run = 0; run < nruns; run++) {
+            const int run0 = run * 32 * kAdjR;
+            f2 T2[kAdjR / 2], S2[kAdjR / 2], MT[kAdjR / 2];
+            float t2min = 3.0e38f, smin = 3.0e38f;
+            bool any = false;
+#pragma unroll
+            for (int h = 0; h < kAdjR / 2; h++) {
+                float tv[2], sv[2], mv[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int l = run0 + lane + 32 * (2 * h + e);
+                    const bool ok = l < g.nz;
+                    const int lc = ok ? l : g.nz - 1;
+                    const float tau = g.z0 + (float)lc * g.dz;
+                    const float tq = tau * invdt;
+                    const float v = a.velCube ? a.vel[(size_t)col * g.nz + lc] : a.vel[lc];
+                    const float vd = v * g.dt;
+                    tv[e] = tq * tq;
+                    sv[e] = 1.0f / (vd * vd);
+                    // |tau| m[p]: the per-image-sample factor of the weight
+                    mv[e] = ok ? fabsf(tau) * a.image[(size_t)col * g.nz + l] : 0.0f;
+                    if (ok) { t2min = fminf(t2min, tv[e]); smin = fminf(smin, sv[e]); }
+                    any |= (mv[e] != 0.0f);
+                }
+                T2[h] = pk(tv[0], tv[1]);
+                S2[h] = pk(sv[0], sv[1]);
+                MT[h] = pk(mv[0], mv[1]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                t2min = fminf(t2min, __shfl_xor_sync(0xffffffffu, t2min, o));
+                smin = fminf(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+            }
+            if (!__any_sync(0xffffffffu, any)) continue;        // zero model in this run
+            for (int c = 0; c < n; c++) {
+                const float mx = crd[c], my = crd[a.chunk + c], ox = crd[2 * a.chunk + c],
+                            oy = crd[3 * a.chunk + c];
+                const float dmx = mx - cx, dmy = my - cy;
+                if (ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2) continue;
+                const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
+                const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
+                // conservative bound (approximate square roots; the margin covers them)
+                const float ulb = sqrt_approx(fmaf(ds, smin, t2min)) + sqrt_approx(fmaf(dr, smin, t2min));
+                if (!(ulb < umax * 1.0001f + 1.0f)) continue;   // past the trace end (warp-uniform)
+                const unsigned rowS = accS + (unsigned)(c * a.pitch) * 4u;
+                const f2 DS = pk(ds, ds), DR = pk(dr, dr);
+                // phase 1: kinematics, weights and contributions of all the lane's pairs
+                // (the table loads pipeline back to back); phase 2: the scatter
+                unsigned adr[kAdjR];
+                float ca[kAdjR], cb[kAdjR];
+#pragma unroll
+                for (int h = 0; h < kAdjR / 2; h++) {
+                    const PairKin kk = pair_kin(DS, DR, S2[h], T2[h], umax, M2);
+                    f2 W;
+                    if (WT == 0) {
+                        const float2 w0 = lds_f2(wS + kk.q0 * 8u), w1 = lds_f2(wS + kk.q1 * 8u);
+                        W = fma2(kk.F, pk(w0.y, w1.y), pk(w0.x, w1.x));
+                    } else {
+                        W = mul2(pk(sqrt_approx(kk.u0), sqrt_approx(kk.u1)),
+                                 pk(sqrtf(g.dt), sqrtf(g.dt)));
+                    }
+                    const f2 VAL = mul2(W, MT[h]);
+                    adr[2 * h] = rowS + kk.q0 * 4u;
+                    adr[2 * h + 1] = rowS + kk.q1 * 4u;
+                    if (PICK == KTM_PICK_LINEAR) {
+                        const f2 B = mul2(VAL, kk.F);          // f * val
+                        const f2 A = sub2(VAL, B);             // (1 - f) * val
+                        upk(A, ca[2 * h], ca[2 * h + 1]);
+                        upk(B, cb[2 * h], cb[2 * h + 1]);
+                    } else {
+                        upk(VAL, ca[2 * h], ca[2 * h + 1]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kAdjR; r++) {
+                    scatter_add(adr[r], ca[r], lane);
+                    if (PICK == KTM_PICK_LINEAR) scatter_add(adr[r] + 4u, cb[r], lane);
+                }
+            }
+        }
+    }
+    asm volatile("" ::: "memory");     // the scatter wrote acc: no load below reuses older values
+    __syncthreads();
+    // out: samples 0 < j < nt; the guards absorbed the pairs that read zero guards
+    for (int i = threadIdx.x; i < n * a.pitch; i += kAdjThreads) {
+        const int c = i / a.pitch, j = i % a.pitch;
+        const float v = (j > 0 && j < g.nt) ? acc[i] : 0.0f;
+        float* dst = a.data + (size_t)(k0 + c) * a.pitch + j;
+        if (a.atomicOut) {
+            if (v != 0.0f) atomicAdd(dst, v);
+        } else {
+            *dst += v;
+        }
+    }
+}
+
+}  // namespace
+
+int launch_demigrate(const Geometry& g, const float* midX, const float* midY, const float* offX,
+                     const float* offY, const float* vel, int velCube, const float* image,
+                     float* data, int pitch, int pick, int weightMethod, float aperture,
+                     int accumulate, cudaStream_t s)
+{
+    if (pitch < g.nt + 2 || pitch % 4 != 0)
+        return set_error(KTM_ERR_ARG, "demigrate: dataPitch must be >= tracePts + 2 and a multiple of 4");
+    const size_t pitchBytes = (size_t)pitch * sizeof(float);
+    if (!accumulate && g.ntr > 0)
+        KTM_CUDA_TRY(cudaMemsetAsync(data, 0, pitchBytes * g.ntr, s));
+    if (g.ntr == 0 || (long long)g.nx * g.ny * g.nz == 0) return KTM_OK;
+    const size_t fixed = (size_t)(g.nt + 1) * sizeof(float2) + 64;
+    const size_t perTrace = pitchBytes + 4 * sizeof(float);
+    int chunk = 32;
+    while (chunk > 1 && fixed + chunk * perTrace > kAdjSmemBudget) chunk--;
+    if (fixed + chunk * perTrace > (size_t)kMaxSmemBytes)
+        return set_error(KTM_ERR_LIMIT, "demigrate: tracePts=%d exceeds the shared-memory limit", g.nt);
+    const size_t smem = fixed + chunk * perTrace;
+
+    int dev = 0, sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    const int ncols = g.nx * g.ny;
+    const int chunks = (g.ntr + chunk - 1) / chunk;
+    // column blocks only when the traces alone give too few CTAs (then the
+    // chunks are added into the data with global atomics)
+    int blocks = 1;
+    const int want = 6 * sm;
+    if (chunks < want) blocks = std::min((want + chunks - 1) / chunks, std::max(1, ncols / 16));
+    const int perBlock = (ncols + blocks - 1) / blocks;
+    blocks = (ncols + perBlock - 1) / perBlock;
+
+    AdjArgs a;
+    a.g = g; a.midX = midX; a.midY = midY; a.offX = offX; a.offY = offY;
+    a.vel = vel; a.velCube = velCube; a.image = image; a.data = data; a.pitch = pitch;
+    a.pick = pick; a.weightMethod = weightMethod; a.aperture = aperture;
+    a.chunk = chunk; a.colsPerBlock = perBlock; a.atomicOut = blocks > 1;
+    dim3 grid((unsigned)chunks, (unsigned)blocks);
+#define KTM_ADJ_LAUNCH(P, W)                                                                    \
+    do {                                                                                        \
+        KTM_CUDA_TRY(cudaFuncSetAttribute(demigrate_kernel<P, W>,                              \
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        demigrate_kernel<P, W><<<grid, kAdjThreads, smem, s>>>(a);                             \
+    } while (0)
+    const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : 0;
+    if (pick == KTM_PICK_LINEAR) {
+        if (wt) KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 1); else KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 0);
+    } else {
+        if (wt) KTM_ADJ_LAUNCH(KTM_PICK_TRUNCATE, 1); else KTM_ADJ_LAUNCH(KTM_PICK_TRUNCATE, 0);
+    }
+#undef KTM_ADJ_LAUNCH
+    KTM_CUDA_TRY(cudaGetLastError());
+    return KTM_OK;
+}
+
+}  // namespace ktm

@@ -338,3 +338,59 @@ int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, doub
 }
 
 }  // extern "C"
+
+namespace ktm {
+int job_geometry(const ktm_job* j, Geometry* g) { return make_geometry(j, g); }
+}  // namespace ktm
+
+extern "C" int ktmDemigrate(const ktm_job* job, float* data, int dataPitch)
+{
+    using namespace ktm;
+    if (!job) return set_error(KTM_ERR_ARG, "NULL job");
+    if (!job->deviceMemory) return set_error(KTM_ERR_ARG, "ktmDemigrate takes device memory");
+    if (job->pick != KTM_PICK_TRUNCATE && job->pick != KTM_PICK_LINEAR)
+        return set_error(KTM_ERR_ARG, "bad pick %d", job->pick);
+    if (job->weightMethod != KTM_WEIGHT_TABLE && job->weightMethod != KTM_WEIGHT_SQRT)
+        return set_error(KTM_ERR_ARG, "bad weightMethod %d", job->weightMethod);
+    Geometry g;
+    int rc = make_geometry(job, &g);
+    if (rc) return rc;
+    const long long nimg = (long long)g.nx * g.ny * g.nz;
+    if (g.ntr > 0 && (!job->midX || !job->midY || !job->offX || !job->offY || !data))
+        return set_error(KTM_ERR_ARG, "NULL coordinate or data pointer");
+    if (nimg > 0 && g.ntr > 0 && (!job->image || !job->velocity))
+        return set_error(KTM_ERR_ARG, "NULL model or velocity");
+    rc = launch_demigrate(g, job->midX, job->midY, job->offX, job->offY, job->velocity,
+                          job->velocityCube, job->image, data, dataPitch, job->pick,
+                          job->weightMethod, job->aperture, job->accumulate,
+                          static_cast<cudaStream_t>(job->stream));
+    return rc ? rc : set_ok();
+}
+
+extern "C" int ktmVrmsGradient(const ktm_job* job, float* grad)
+{
+    using namespace ktm;
+    if (!job) return set_error(KTM_ERR_ARG, "NULL job");
+    if (!job->deviceMemory || !job->tracesPacked)
+        return set_error(KTM_ERR_ARG, "ktmVrmsGradient takes device memory and a packed trace set");
+    int rc = check_job(job);
+    if (rc) return rc;
+    Geometry g;
+    rc = make_geometry(job, &g);
+    if (rc) return rc;
+    if (!grad && (long long)g.nx * g.ny * g.nz > 0) return set_error(KTM_ERR_ARG, "NULL grad");
+    if (!job->traceScale) return set_error(KTM_ERR_ARG, "packed traces need traceScale");
+    FastArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = g; a.midX = job->midX; a.midY = job->midY; a.offX = job->offX; a.offY = job->offY;
+    a.traces = job->traces; a.scale = job->traceScale; a.fmt = job->traceFormat; a.pitch = g.stride;
+    a.weightMode = job->tracesPrefolded ? 2 : 0;
+    a.weightMethod = job->weightMethod;
+    a.vel = job->velocity; a.velCube = job->velocityCube;
+    a.image = grad; a.accumulate = 0;
+    a.pick = job->pick; a.aperture = job->aperture;
+    a.tileRun = job->tileRun;
+    a.grad = 1;
+    rc = launch_fast(a, static_cast<cudaStream_t>(job->stream));
+    return rc ? rc : set_ok();
+}

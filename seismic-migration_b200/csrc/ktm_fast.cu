@@ -33,167 +33,15 @@
 //   column) the squared distances and a skip flag (aperture, or a lower bound
 //   of u over the run beyond the trace end), so the inner loop branches once
 //   per trace, warp-uniformly.
-#include "ktm_internal.cuh"
-
-#include <cuda_bf16.h>
-#include <cuda_fp16.h>
+#include "ktm_pair.cuh"
 
 namespace ktm {
 namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
-constexpr int kMagicBits = 0x4B400000;
 constexpr size_t kFastSmemBudget = 110 * 1024;   // two CTAs per SM
-
-// ------------------------------------------------------------- f32x2 PTX ---
-struct f2 {
-    unsigned long long v;
-};
-__device__ __forceinline__ f2 pk(float a, float b)
-{
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ void upk(f2 x, float& a, float& b)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
-{
-    f2 r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-    return r;
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b)
-{
-    f2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-    return r;
-}
-__device__ __forceinline__ f2 add2_rm(f2 a, f2 b)
-{
-    f2 r;
-    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-    return r;
-}
-__device__ __forceinline__ f2 sub2(f2 a, f2 b)
-{
-    f2 r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-    return r;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b)
-{
-    f2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-    return r;
-}
-
-__device__ __forceinline__ float sqrt_approx(float x)
-{
-    float y;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// packed sample element -> float
-template <int FMT> struct Elem;
-template <> struct Elem<KTM_FMT_F32> {
-    using T = float;
-    static __device__ __forceinline__ float get(const T* p, int i) { return p[i]; }
-};
-template <> struct Elem<KTM_FMT_BF16> {
-    using T = unsigned short;
-    static __device__ __forceinline__ float get(const T* p, int i)
-    {
-        return __uint_as_float(static_cast<unsigned>(p[i]) << 16);
-    }
-};
-template <> struct Elem<KTM_FMT_F16> {
-    using T = __half;
-    static __device__ __forceinline__ float get(const T* p, int i) { return __half2float(p[i]); }
-};
-
-// Shared-memory loads through 32-bit shared addresses.  The sample index comes
-// out of the round-down magic add as bits(fl) = 0x4B400000 + i0, so the row
-// base is pre-offset by -0x4B400000 * sizeof(T) (mod 2^32) and the address is
-// one multiply-add of the float's bits.  Volatile: these loads must stay
-// between the barriers that bracket each chunk.
-template <int FMT> struct Lds;
-template <> struct Lds<KTM_FMT_F32> {
-    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
-    {
-        asm volatile("ld.shared.f32 %0, [%2];\n\tld.shared.f32 %1, [%2+4];" : "=f"(a), "=f"(b) : "r"(ad));
-    }
-    static __device__ __forceinline__ float one(unsigned ad)
-    {
-        float a;
-        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(a) : "r"(ad));
-        return a;
-    }
-};
-template <> struct Lds<KTM_FMT_BF16> {
-    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
-    {
-        unsigned short x, y;
-        asm volatile("ld.shared.u16 %0, [%2];\n\tld.shared.u16 %1, [%2+2];" : "=h"(x), "=h"(y) : "r"(ad));
-        a = __uint_as_float(static_cast<unsigned>(x) << 16);
-        b = __uint_as_float(static_cast<unsigned>(y) << 16);
-    }
-    static __device__ __forceinline__ float one(unsigned ad)
-    {
-        unsigned short x;
-        asm volatile("ld.shared.u16 %0, [%1];" : "=h"(x) : "r"(ad));
-        return __uint_as_float(static_cast<unsigned>(x) << 16);
-    }
-};
-template <> struct Lds<KTM_FMT_F16> {
-    static __device__ __forceinline__ void pair(unsigned ad, float& a, float& b)
-    {
-        unsigned short x, y;
-        asm volatile("ld.shared.b16 %0, [%2];\n\tld.shared.b16 %1, [%2+2];" : "=h"(x), "=h"(y) : "r"(ad));
-        a = __half2float(__ushort_as_half(x));
-        b = __half2float(__ushort_as_half(y));
-    }
-    static __device__ __forceinline__ float one(unsigned ad)
-    {
-        unsigned short x;
-        asm volatile("ld.shared.b16 %0, [%1];" : "=h"(x) : "r"(ad));
-        return __half2float(__ushort_as_half(x));
-    }
-};
-__device__ __forceinline__ float2 lds_f2(unsigned ad)
-{
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(ad));
-    return v;
-}
-__device__ __forceinline__ unsigned smem_u32(const void* p)
-{
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
-{
-    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n"); }
-
-struct ColInfo {
-    float x, y;       // column coordinates
-    float t2min;      // min over the run of (tau/dt)^2
-    float smin;       // min over the run of S' = 1/(v dt)^2; < 0: column outside the image
-};
+using namespace dev;
 
 struct ChunkSmem {
     // layout of one CTA's dynamic shared memory
@@ -222,7 +70,7 @@ __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch,
 //   kWtSqrt    a third sqrt.approx per pair on the special-function unit.
 constexpr int kWtTable = 0, kWtPrefold = 1, kWtSqrt = 2;
 
-template <int R, int PICK, int FMT, int PRE>
+template <int R, int PICK, int FMT, int PRE, int GRAD>
 __global__ void __launch_bounds__(kThreads, 2)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
@@ -360,23 +208,50 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                 const f2 DS = pk(gd.x, gd.x), DR = pk(gd.y, gd.y), SC = pk(gd.z, gd.z);
 #pragma unroll
                 for (int h = 0; h < R / 2; h++) {
-                    float as0, as1, ar0, ar1;
-                    upk(fma2(DS, S2[h], T2[h]), as0, as1);
-                    upk(fma2(DR, S2[h], T2[h]), ar0, ar1);
-                    f2 U = add2(pk(sqrt_approx(as0), sqrt_approx(as1)),
-                                pk(sqrt_approx(ar0), sqrt_approx(ar1)));
-                    float u0, u1;
-                    upk(U, u0, u1);
-                    u0 = fminf(u0, umax);
-                    u1 = fminf(u1, umax);
-                    U = pk(u0, u1);
-                    const f2 FL = add2_rm(U, M2);
-                    float fl0, fl1;
-                    upk(FL, fl0, fl1);
-                    const unsigned q0 = __float_as_uint(fl0), q1 = __float_as_uint(fl1);
+                    if (GRAD) {
+                        // d/dS' of |tau| s_k W(u) V(u), u = sqrt(a_s) + sqrt(a_r):
+                        // (dW/du V + W dV/du) du/dS', du/dS' = Ds/(2 sqrt a_s) + Dr/(2 sqrt a_r)
+                        float as0, as1, ar0, ar1;
+                        upk(fma2(DS, S2[h], T2[h]), as0, as1);
+                        upk(fma2(DR, S2[h], T2[h]), ar0, ar1);
+                        const f2 RS = pk(fminf(rsqrt_approx(as0), 3.0e38f), fminf(rsqrt_approx(as1), 3.0e38f));
+                        const f2 RR = pk(fminf(rsqrt_approx(ar0), 3.0e38f), fminf(rsqrt_approx(ar1), 3.0e38f));
+                        f2 U = fma2(pk(ar0, ar1), RR, mul2(pk(as0, as1), RS));
+                        float u0, u1;
+                        upk(U, u0, u1);
+                        u0 = fminf(u0, umax);
+                        u1 = fminf(u1, umax);
+                        U = pk(u0, u1);
+                        const f2 FL = add2_rm(U, M2);
+                        float fl0, fl1;
+                        upk(FL, fl0, fl1);
+                        const unsigned q0 = __float_as_uint(fl0), q1 = __float_as_uint(fl1);
+                        const f2 F = sub2(U, sub2(FL, M2));
+                        const f2 DUDS = mul2(pk(0.5f, 0.5f), fma2(DS, RS, mul2(DR, RR)));
+                        float a0, b0, a1, b1;
+                        Lds<FMT>::pair(rowS + q0 * (unsigned)sizeof(T), a0, b0);
+                        Lds<FMT>::pair(rowS + q1 * (unsigned)sizeof(T), a1, b1);
+                        const f2 A = pk(a0, a1);
+                        const f2 DV = sub2(pk(b0, b1), A);
+                        f2 TERM;
+                        if (PRE == kWtPrefold) {
+                            TERM = DV;
+                        } else {
+                            const float2 w0 = lds_f2(wS + q0 * 8u), w1 = lds_f2(wS + q1 * 8u);
+                            const f2 DW = pk(w0.y, w1.y);
+                            const f2 W = fma2(F, DW, pk(w0.x, w1.x));
+                            const f2 V = fma2(F, DV, A);
+                            TERM = fma2(DW, V, mul2(W, DV));
+                        }
+                        acc[h] = fma2(mul2(SC, TERM), DUDS, acc[h]);
+                        continue;
+                    }
+                    const PairKin kk = pair_kin(DS, DR, S2[h], T2[h], umax, M2);
+                    const f2 F = kk.F;
+                    const float u0 = kk.u0, u1 = kk.u1;
+                    const unsigned q0 = kk.q0, q1 = kk.q1;
                     const unsigned ad0 = rowS + q0 * (unsigned)sizeof(T);
                     const unsigned ad1 = rowS + q1 * (unsigned)sizeof(T);
-                    const f2 F = sub2(U, sub2(FL, M2));
                     f2 V;
                     if (PICK == KTM_PICK_LINEAR) {
                         float a0, b0, a1, b1;
@@ -409,14 +284,17 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                              : a.image + (size_t)col * g.nz;
 #pragma unroll
         for (int h = 0; h < R / 2; h++) {
-            float v2[2];
+            float v2[2], s2[2];
             upk(acc[h], v2[0], v2[1]);
+            upk(S2[h], s2[0], s2[1]);
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 const int l = run0 + lane + 32 * (2 * h + e);
                 if (l < g.nz) {
                     const float tau = fabsf(g.z0 + (float)l * g.dz);
-                    const float v = v2[e] * (PRE == kWtSqrt ? tau * sqrtf(g.dt) : tau);
+                    // GRAD: dI/dv = dI/dS' dS'/dv, S' = 1/(v dt)^2, dS'/dv = -2 dt S'^(3/2)
+                    const float gfac = GRAD ? -2.0f * g.dt * s2[e] * sqrtf(s2[e]) : 1.0f;
+                    const float v = v2[e] * gfac * (PRE == kWtSqrt ? tau * sqrtf(g.dt) : tau);
                     out[l] = (!partial && a.accumulate) ? out[l] + v : v;
                 }
             }
@@ -437,7 +315,7 @@ __global__ void reduce_slices(float* __restrict__ out, const float* __restrict__
     }
 }
 
-template <int R, int PICK, int FMT, int PRE>
+template <int R, int PICK, int FMT, int PRE, int GRAD>
 int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const Geometry& g = a.g;
@@ -448,7 +326,7 @@ int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
         return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
                                         "stage limit", a.pitch);
     const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt).total;
-    auto kern = fast_kernel<R, PICK, FMT, PRE>;
+    auto kern = fast_kernel<R, PICK, FMT, PRE, GRAD>;
     KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     const long long cols = (long long)g.nx * g.ny;
@@ -491,19 +369,27 @@ int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
     return KTM_OK;
 }
 
-template <int R, int PICK, int PRE>
+template <int R, int PICK, int PRE, int GRAD = 0>
 int launch_fmt(const FastArgs& a, cudaStream_t s, int sm)
 {
     switch (a.fmt) {
-        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32, PRE>(a, s, sm);
-        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16, PRE>(a, s, sm);
-        default: return launch_t<R, PICK, KTM_FMT_BF16, PRE>(a, s, sm);
+        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32, PRE, GRAD>(a, s, sm);
+        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16, PRE, GRAD>(a, s, sm);
+        default: return launch_t<R, PICK, KTM_FMT_BF16, PRE, GRAD>(a, s, sm);
     }
 }
 
 template <int R>
 int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
 {
+    if (a.grad) {
+        // velocity gradient: linear pick; table weight or prefolded samples
+        if (a.pick != KTM_PICK_LINEAR || (a.weightMode != 2 && a.weightMethod != KTM_WEIGHT_TABLE))
+            return set_error(KTM_ERR_ARG, "ktmVrmsGradient takes the linear pick with the table "
+                                          "weight or prefolded samples");
+        return a.weightMode == 2 ? launch_fmt<R, KTM_PICK_LINEAR, kWtPrefold, 1>(a, s, sm)
+                                 : launch_fmt<R, KTM_PICK_LINEAR, kWtTable, 1>(a, s, sm);
+    }
     // a.weightMode: 2 samples prefolded; otherwise a.weightMethod picks table / sqrt
     if (a.weightMode == 2) {
         if (a.pick != KTM_PICK_LINEAR)

@@ -58,6 +58,7 @@ struct FastArgs {
     int pick; float aperture;
     int tileRun, tileCols;
     int slices;             // trace slices (0: chosen to fill the GPU)
+    int grad;               // 1: write dI/dv (velocity gradient) instead of the image
     void* scratch;          // optional preallocated partial-image buffer
     size_t scratchBytes;
     unsigned long long* pairsEvaluated;
@@ -65,6 +66,15 @@ struct FastArgs {
 // Fast kernel on a PACKED trace set (ktmPrepareTraces layout); linear pick
 // expects samples prefolded with sqrt(j*dt), truncating pick expects them not.
 int launch_fast(const FastArgs& a, cudaStream_t stream);
+
+// ktm_adjoint.cu: demigration into the packed F32 layout [ntr][pitch]
+int launch_demigrate(const Geometry& g, const float* midX, const float* midY, const float* offX,
+                     const float* offY, const float* vel, int velCube, const float* image,
+                     float* data, int pitch, int pick, int weightMethod, float aperture,
+                     int accumulate, cudaStream_t s);
+
+// ktm_api.cu: geometry of a job (validates sizes)
+int job_geometry(const ktm_job* j, Geometry* g);
 
 // ktm_prep.cu
 int packed_pitch(int nt, int fmt);

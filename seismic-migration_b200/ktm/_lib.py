@@ -82,6 +82,15 @@ class KtmPrep(C.Structure):
     ]
 
 
+class KtmLsm(C.Structure):
+    """ktm_lsm (include/ktm.h)."""
+    _fields_ = [
+        ("job", KtmJob), ("data", P), ("dataPitch", C.c_int), ("model", P),
+        ("iterations", C.c_int), ("useGraph", C.c_int), ("residualNorms", P),
+        ("gradientNorms", P),
+    ]
+
+
 _lib = None
 
 
@@ -118,6 +127,12 @@ def lib() -> C.CDLL:
     L.ktmPackedPitch.restype = C.c_int
     L.ktmPrepareTraces.argtypes = [C.POINTER(KtmPrep)]
     L.ktmPrepareTraces.restype = C.c_int
+    L.ktmDemigrate.argtypes = [C.POINTER(KtmJob), P, C.c_int]
+    L.ktmDemigrate.restype = C.c_int
+    L.ktmVrmsGradient.argtypes = [C.POINTER(KtmJob), P]
+    L.ktmVrmsGradient.restype = C.c_int
+    L.ktmLeastSquaresMigrate.argtypes = [C.POINTER(KtmLsm)]
+    L.ktmLeastSquaresMigrate.restype = C.c_int
     L.ktmMigratePackedNoAlloc.argtypes = [C.POINTER(KtmJob)]
     L.ktmMigratePackedNoAlloc.restype = C.c_int
     L.ktmProbePeaks.argtypes = [P, P, P]

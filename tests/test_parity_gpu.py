@@ -149,7 +149,11 @@ def test_fast_linear_matches_f64_oracle(cuda, ktm_lib, seed):
 
 
 def test_fast_truncate_matches_f64_oracle(cuda, ktm_lib):
-    case = random_case(7, ntr=90, nz=200, data="ricker")
+    # tau step incommensurate with dt: with dz = dt/2 every zero-offset pair has an
+    # exactly integer t/dt, and FP32 rounding then truncates about half of them one
+    # sample lower (1e-2 relative L2 in an FP32 emulation; the reference's own FP32
+    # code does the same, and reference mode matches it bit for bit)
+    case = random_case(7, ntr=90, nz=200, dz=0.00173, data="ricker")
     img = fast(cuda, case, pick="truncate")
     ref = oracle.migrate_f64(*case, pick=0, prefold=3)
     # A truncated index flips where t/dt is within the FP32 / sqrt.approx error
@@ -333,7 +337,7 @@ def test_fast_packed_table_weight_gate(cuda, ktm_lib, fmt):
 @pytest.mark.parametrize("pick", ["linear", "truncate"])
 def test_fast_sqrt_weight_matches_reference_weight(cuda, ktm_lib, pick):
     """weightMethod = SQRT: the reference weight |tau| sqrt(t) per pair."""
-    case = random_case(15, ntr=150, nz=260, data="ricker")
+    case = random_case(15, ntr=150, nz=260, dz=0.00173, data="ricker")
     img = fast(cuda, case, pick=pick, weight="sqrt")
     ref = oracle.migrate_f64(*case, pick=1 if pick == "linear" else 0, prefold=0)
     assert rel_l2(img, ref) < (2e-5 if pick == "linear" else TRUNC_GATE)
