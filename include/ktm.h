@@ -260,6 +260,25 @@ typedef struct ktm_lsm {
 } ktm_lsm;
 int ktmLeastSquaresMigrate(const ktm_lsm* lsm);
 
+/* ------------------------------------------------------------------------ */
+/* Batched target-oriented migration and tile tuning                        */
+/* (no counterpart in the reference)                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Many independent jobs (image patches of any size, trace sets of any size) in
+ * ONE persistent launch: a queue of (job, 8 image columns, tau run, trace slice)
+ * tiles sorted longest first, pulled by one CTA per SM slot.  Every job: FAST
+ * mode, device memory, a packed trace set; all jobs share the trace format,
+ * pick and weight, and the first job's tileRun (0: chosen from the jobs' Nz).
+ * Images are overwritten.  Asynchronous on `stream`. */
+int ktmMigrateBatch(const ktm_job* jobs, int njobs, void* stream);
+
+/* Tile tuning: times the fast kernel's tau-run length (256, 384, 512 samples per
+ * warp) on up to 4096 of the job's traces and returns the fastest in *tileRun
+ * (remembered per image / trace shape, format, pick and weight for the process).
+ * Overwrites job->image.  Device memory, packed traces; synchronous. */
+int ktmAutotune(const ktm_job* job, int* tileRun);
+
 /* ktmMigrate for callers that cannot allocate device memory while they run:
  * a processing loop that must never let cudaMalloc / cudaFree synchronise the
  * device, or a host framework that has already shared the GPU's memory out

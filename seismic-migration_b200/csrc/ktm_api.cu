@@ -2,8 +2,11 @@
 // replace ktmMigrationCPU / ktmMigrationGPU, and the extended job API.
 #include "ktm_internal.cuh"
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace ktm {
@@ -393,4 +396,117 @@ extern "C" int ktmVrmsGradient(const ktm_job* job, float* grad)
     a.grad = 1;
     rc = launch_fast(a, static_cast<cudaStream_t>(job->stream));
     return rc ? rc : set_ok();
+}
+
+namespace ktm {
+namespace {
+
+// FastArgs of a device-memory FAST job on a packed trace set.
+int packed_args(const ktm_job* j, FastArgs* a)
+{
+    if (!j) return set_error(KTM_ERR_ARG, "NULL job");
+    if (!j->deviceMemory || !j->tracesPacked || j->mode != KTM_MODE_FAST)
+        return set_error(KTM_ERR_ARG, "batched and tuned launches take FAST mode, device memory "
+                                      "and packed traces");
+    int rc = check_job(j);
+    if (rc) return rc;
+    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
+        return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
+    std::memset(a, 0, sizeof(*a));
+    rc = make_geometry(j, &a->g);
+    if (rc) return rc;
+    if (!j->traceScale && j->config.traceNo > 0) return set_error(KTM_ERR_ARG, "packed traces need traceScale");
+    a->midX = j->midX; a->midY = j->midY; a->offX = j->offX; a->offY = j->offY;
+    a->traces = j->traces; a->scale = j->traceScale; a->fmt = j->traceFormat; a->pitch = a->g.stride;
+    a->weightMode = j->tracesPrefolded ? 2 : 0;
+    a->weightMethod = j->weightMethod;
+    a->vel = j->velocity; a->velCube = j->velocityCube;
+    a->image = j->image; a->accumulate = j->accumulate;
+    a->pick = j->pick; a->aperture = j->aperture;
+    a->tileRun = j->tileRun;
+    a->pairsEvaluated = j->pairsEvaluated;
+    return KTM_OK;
+}
+
+struct TuneKey {
+    int nx, ny, nz, nt, fmt, pick, weightMode, weightMethod;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::memcmp(this, &o, sizeof(TuneKey)) < 0;
+    }
+};
+std::mutex g_tuneMu;
+std::map<TuneKey, int> g_tuned;
+
+}  // namespace
+}  // namespace ktm
+
+extern "C" int ktmMigrateBatch(const ktm_job* jobs, int njobs, void* stream)
+{
+    using namespace ktm;
+    if (njobs < 0 || (njobs > 0 && !jobs)) return set_error(KTM_ERR_ARG, "bad job list");
+    std::vector<FastArgs> args(njobs);
+    for (int j = 0; j < njobs; j++) {
+        int rc = packed_args(&jobs[j], &args[j]);
+        if (rc) return rc;
+        if (!jobs[j].image && (long long)args[j].g.nx * args[j].g.ny * args[j].g.nz > 0)
+            return set_error(KTM_ERR_ARG, "job %d: NULL image", j);
+    }
+    int rc = launch_batch(args.data(), njobs, static_cast<cudaStream_t>(stream));
+    return rc ? rc : set_ok();
+}
+
+extern "C" int ktmAutotune(const ktm_job* job, int* tileRun)
+{
+    using namespace ktm;
+    if (!tileRun) return set_error(KTM_ERR_ARG, "NULL tileRun");
+    FastArgs a;
+    int rc = packed_args(job, &a);
+    if (rc) return rc;
+    TuneKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.nx = a.g.nx; key.ny = a.g.ny; key.nz = a.g.nz; key.nt = a.g.nt; key.fmt = a.fmt;
+    key.pick = a.pick; key.weightMode = a.weightMode; key.weightMethod = a.weightMethod;
+    {
+        std::lock_guard<std::mutex> lock(g_tuneMu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            *tileRun = it->second;
+            return set_ok();
+        }
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(job->stream);
+    // time each run length on a sample of the traces (the image is overwritten)
+    a.g.ntr = std::min(a.g.ntr, 4096);
+    a.accumulate = 0;
+    a.pairsEvaluated = nullptr;
+    cudaEvent_t e0, e1;
+    KTM_CUDA_TRY(cudaEventCreate(&e0));
+    KTM_CUDA_TRY(cudaEventCreate(&e1));
+    int best = 0;
+    float bestMs = 3.0e38f;
+    for (int run : {256, 384, 512}) {
+        a.tileRun = run;
+        if ((rc = launch_fast(a, s))) break;               // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 2 && !rc; r++) rc = launch_fast(a, s);
+        cudaEventRecord(e1, s);
+        if (rc) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = set_error(KTM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < bestMs) { bestMs = ms; best = run; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lock(g_tuneMu);
+        g_tuned[key] = best;
+    }
+    *tileRun = best;
+    return set_ok();
 }

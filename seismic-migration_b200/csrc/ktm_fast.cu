@@ -35,6 +35,9 @@
 //   per trace, warp-uniformly.
 #include "ktm_pair.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace ktm {
 namespace {
 
@@ -70,27 +73,33 @@ __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch,
 //   kWtSqrt    a third sqrt.approx per pair on the special-function unit.
 constexpr int kWtTable = 0, kWtPrefold = 1, kWtSqrt = 2;
 
+// Output of a tile: the image (overwrite or accumulate), one trace slice's partial
+// image, or atomic adds into the image (tiles of the batched launch).
+enum { kOutImage = 0, kOutPartial = 1, kOutAtomic = 2 };
+
+// One CTA-tile of the gather: image columns [colGroup*8, colGroup*8+8) x the tau
+// run runIdx x traces [kb, ke).  Used by the grid launch (one tile per CTA) and
+// by the persistent batched launch (a queue of tiles from many jobs).
 template <int R, int PICK, int FMT, int PRE, int GRAD>
-__global__ void __launch_bounds__(kThreads, 2)
-fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
+__device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colGroup, int runIdx,
+                                          int kb, int ke, float* __restrict__ partial, int outMode,
+                                          unsigned char* smem_raw, ColInfo* cinfo)
 {
     static_assert(R % 2 == 0, "R pairs");
     using T = typename Elem<FMT>::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const Geometry& g = a.g;
     const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt);
     T* rawBase = reinterpret_cast<T*>(smem_raw);
     float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
     float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
     float2* wtab = reinterpret_cast<float2*>(smem_raw + L.wtabOff);
-    __shared__ ColInfo cinfo[kWarps];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ncols = g.nx * g.ny;
-    const int col = blockIdx.x * kWarps + warp;
+    const int col = colGroup * kWarps + warp;
     const bool colValid = col < ncols;
     const int ci = colValid ? col / g.ny : 0, cj = colValid ? col % g.ny : 0;
-    const int run0 = blockIdx.y * (32 * R);
+    const int run0 = runIdx * (32 * R);
     const float invdt = 1.0f / g.dt;
 
     // ---- per-thread tau tables, two tau samples per packed register pair ----
@@ -135,8 +144,6 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
         }
     }
 
-    const int kb = blockIdx.z * perSlice;
-    const int ke = min(g.ntr, kb + perSlice);
     const int nchunks = ke > kb ? (ke - kb + chunk - 1) / chunk : 0;
     const size_t rowBytes = (size_t)a.pitch * sizeof(T);
 
@@ -160,7 +167,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
     const float umax = (float)g.nt;
     const float ap2 = a.aperture > 0.0f ? a.aperture * a.aperture : -1.0f;
     const f2 M2 = pk(kMagic, kMagic);
-    unsigned long long evaluated = 0;
+    unsigned keptTraces = 0;        // traces this warp evaluated (all lanes agree)
 
     if (nchunks > 0) issue(0);
     for (int ch = 0; ch < nchunks; ch++) {
@@ -185,8 +192,9 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                     bool keep = !(ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2);
                     if (keep) {
                         // lower bound of u over the run: past the last sample -> no contribution
-                        const float ulb = sqrtf(fmaf(ds, cw.smin, cw.t2min)) +
-                                          sqrtf(fmaf(dr, cw.smin, cw.t2min));
+                        // approximate square roots: the margin below covers their error
+                        const float ulb = sqrt_approx(fmaf(ds, cw.smin, cw.t2min)) +
+                                          sqrt_approx(fmaf(dr, cw.smin, cw.t2min));
                         keep = ulb < umax * 1.0001f + 1.0f;
                     }
                     if (keep) gd = make_float4(ds, dr, sc, 0.0f);
@@ -203,7 +211,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
             for (int c = 0; c < n; c++) {
                 const float4 gd = geo[c * kWarps + warp];
                 if (gd.x < 0.0f) continue;                 // warp-uniform
-                evaluated += nvalid;
+                keptTraces++;
                 const unsigned rowS = rowsS + (unsigned)(c * a.pitch) * (unsigned)sizeof(T) - magicT;
                 const f2 DS = pk(gd.x, gd.x), DR = pk(gd.y, gd.y), SC = pk(gd.z, gd.z);
 #pragma unroll
@@ -279,9 +287,7 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
     }
 
     if (colValid) {
-        const size_t nimg = (size_t)ncols * g.nz;
-        float* out = partial ? partial + blockIdx.z * nimg + (size_t)col * g.nz
-                             : a.image + (size_t)col * g.nz;
+        float* out = (outMode == kOutPartial ? partial : a.image) + (size_t)col * g.nz;
 #pragma unroll
         for (int h = 0; h < R / 2; h++) {
             float v2[2], s2[2];
@@ -295,12 +301,64 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
                     // GRAD: dI/dv = dI/dS' dS'/dv, S' = 1/(v dt)^2, dS'/dv = -2 dt S'^(3/2)
                     const float gfac = GRAD ? -2.0f * g.dt * s2[e] * sqrtf(s2[e]) : 1.0f;
                     const float v = v2[e] * gfac * (PRE == kWtSqrt ? tau * sqrtf(g.dt) : tau);
-                    out[l] = (!partial && a.accumulate) ? out[l] + v : v;
+                    if (outMode == kOutAtomic) atomicAdd(out + l, v);
+                    else out[l] = (outMode == kOutImage && a.accumulate) ? out[l] + v : v;
                 }
             }
         }
     }
-    if (a.pairsEvaluated && lane == 0 && evaluated) atomicAdd(a.pairsEvaluated, evaluated);
+    if (a.pairsEvaluated && lane == 0 && keptTraces)
+        atomicAdd(a.pairsEvaluated, (unsigned long long)keptTraces * (unsigned long long)nvalid);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent batched launch: one CTA per SM slot pulls (job, column group, tau
+// run, trace slice) tiles from a queue sorted longest first; each tile adds its
+// result into its job's image with atomics (the images start at zero).  The
+// job's arguments are copied into shared memory for the tile.
+// ---------------------------------------------------------------------------
+struct BatchTile {
+    int job, cg, run, kb, ke, pad;
+};
+
+template <int R, int PICK, int FMT, int PRE>
+__global__ void __launch_bounds__(kThreads, 2)
+batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
+             const BatchTile* __restrict__ tiles, int ntiles, unsigned* __restrict__ counter)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ColInfo cinfo[kWarps];
+    __shared__ FastArgs sa;
+    __shared__ int st;
+    static_assert(sizeof(FastArgs) % 4 == 0, "word copy");
+    for (;;) {
+        if (threadIdx.x == 0) st = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int t = st;
+        if (t >= ntiles) break;                    // every thread read the same t
+        const BatchTile tl = tiles[t];
+        const int* src = reinterpret_cast<const int*>(jobs + tl.job);
+        int* dst = reinterpret_cast<int*>(&sa);
+        for (int i = threadIdx.x; i < (int)(sizeof(FastArgs) / 4); i += kThreads) dst[i] = src[i];
+        __syncthreads();
+        fast_tile<R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke, nullptr,
+                                        kOutAtomic, smem_raw, cinfo);
+        __syncthreads();                           // shared memory is reused by the next tile
+    }
+}
+
+template <int R, int PICK, int FMT, int PRE, int GRAD>
+__global__ void __launch_bounds__(kThreads, 2)
+fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ColInfo cinfo[kWarps];
+    const int kb = blockIdx.z * perSlice;
+    const int ke = min(a.g.ntr, kb + perSlice);
+    const size_t nimg = (size_t)a.g.nx * a.g.ny * a.g.nz;
+    fast_tile<R, PICK, FMT, PRE, GRAD>(a, chunk, blockIdx.x, blockIdx.y, kb, ke,
+                                       partial ? partial + blockIdx.z * nimg : nullptr,
+                                       partial ? kOutPartial : kOutImage, smem_raw, cinfo);
 }
 
 // out[i] = (accumulate ? out[i] : 0) + sum_z partial[z][i], z in increasing order
@@ -515,6 +573,162 @@ int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* ou
     f64_kernel<<<(unsigned)((n + th - 1) / th), th, 0, stream>>>(a, cols, ncols, out);
     KTM_CUDA_TRY(cudaGetLastError());
     return KTM_OK;
+}
+
+}  // namespace ktm
+
+namespace ktm {
+namespace {
+
+template <int R, int PICK, int FMT, int PRE>
+int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
+{
+    const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
+    int dev = 0, sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = 2 * sm;
+    std::vector<int> chunks(njobs);
+    size_t smem = 0;
+    double totalPairs = 0.0;
+    for (int j = 0; j < njobs; j++) {
+        const Geometry& g = jobs[j].g;
+        int c = 32;
+        while (c > 1 && chunk_layout(c, jobs[j].pitch, esize, g.nt).total > kFastSmemBudget) c--;
+        const size_t need = chunk_layout(c, jobs[j].pitch, esize, g.nt).total;
+        if (need > (size_t)kMaxSmemBytes)
+            return set_error(KTM_ERR_LIMIT, "batch: job %d packed pitch %d exceeds shared memory", j,
+                             jobs[j].pitch);
+        chunks[j] = c;
+        smem = std::max(smem, need);
+        totalPairs += (double)g.nx * g.ny * g.nz * g.ntr;
+    }
+    // tiles: every job's column groups x tau runs, traces sliced so that no tile
+    // exceeds ~1/16 of a CTA's share of the whole batch
+    const double perTile = std::max(1.0, totalPairs / (ctas * 16.0));
+    std::vector<BatchTile> tiles;
+    std::vector<double> cost;
+    for (int j = 0; j < njobs; j++) {
+        const Geometry& g = jobs[j].g;
+        const long long cols = (long long)g.nx * g.ny;
+        if (cols * g.nz == 0 || g.ntr == 0) continue;
+        const int cgs = (int)((cols + kWarps - 1) / kWarps);
+        const int runs = (g.nz + 32 * R - 1) / (32 * R);
+        const double tilePairsPerTrace = (double)kWarps * 32 * R;
+        int per = (int)std::min<double>(g.ntr, std::max<double>(4.0 * chunks[j], perTile / tilePairsPerTrace));
+        per = std::max(per, 1);
+        for (int cg = 0; cg < cgs; cg++)
+            for (int r = 0; r < runs; r++)
+                for (int kb = 0; kb < g.ntr; kb += per) {
+                    const int ke = std::min(g.ntr, kb + per);
+                    tiles.push_back(BatchTile{j, cg, r, kb, ke, 0});
+                    cost.push_back(tilePairsPerTrace * (ke - kb));
+                }
+    }
+    for (int j = 0; j < njobs; j++) {
+        const Geometry& g = jobs[j].g;
+        const size_t nimg = (size_t)g.nx * g.ny * g.nz;
+        if (nimg) KTM_CUDA_TRY(cudaMemsetAsync(jobs[j].image, 0, nimg * sizeof(float), s));
+    }
+    if (tiles.empty()) return KTM_OK;
+    // longest first, so that the queue's tail is made of short tiles
+    std::vector<int> order(tiles.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<BatchTile> sorted(tiles.size());
+    for (size_t i = 0; i < order.size(); i++) sorted[i] = tiles[order[i]];
+
+    const size_t bJobs = sizeof(FastArgs) * njobs, bChunks = sizeof(int) * njobs;
+    const size_t bTiles = sizeof(BatchTile) * sorted.size();
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    unsigned char* buf = nullptr;
+    KTM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&buf), up(bJobs) + up(bChunks) + up(bTiles) + 256, s));
+    FastArgs* dJobs = reinterpret_cast<FastArgs*>(buf);
+    int* dChunks = reinterpret_cast<int*>(buf + up(bJobs));
+    BatchTile* dTiles = reinterpret_cast<BatchTile*>(buf + up(bJobs) + up(bChunks));
+    unsigned* dCounter = reinterpret_cast<unsigned*>(buf + up(bJobs) + up(bChunks) + up(bTiles));
+    cudaError_t e = cudaMemcpyAsync(dJobs, jobs, bJobs, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dChunks, chunks.data(), bChunks, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dTiles, sorted.data(), bTiles, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dCounter, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(batch_kernel<R, PICK, FMT, PRE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+        const int grid = (int)std::min<size_t>((size_t)ctas, sorted.size());
+        batch_kernel<R, PICK, FMT, PRE><<<grid, kThreads, smem, s>>>(dJobs, dChunks, dTiles,
+                                                                      (int)sorted.size(), dCounter);
+        e = cudaGetLastError();
+    }
+    // the host vectors above are pageable: these copies completed before returning
+    cudaFreeAsync(buf, s);
+    if (e != cudaSuccess) return set_error(KTM_ERR_CUDA, "batch launch: %s", cudaGetErrorString(e));
+    return KTM_OK;
+}
+
+template <int R, int PICK, int PRE>
+int launch_batch_fmt(const FastArgs* jobs, int n, cudaStream_t s)
+{
+    switch (jobs[0].fmt) {
+        case KTM_FMT_F32: return launch_batch_t<R, PICK, KTM_FMT_F32, PRE>(jobs, n, s);
+        case KTM_FMT_F16: return launch_batch_t<R, PICK, KTM_FMT_F16, PRE>(jobs, n, s);
+        default: return launch_batch_t<R, PICK, KTM_FMT_BF16, PRE>(jobs, n, s);
+    }
+}
+
+template <int R>
+int launch_batch_r(const FastArgs* jobs, int n, cudaStream_t s)
+{
+    const FastArgs& a = jobs[0];
+    if (a.weightMode == 2) {
+        if (a.pick != KTM_PICK_LINEAR)
+            return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
+        return launch_batch_fmt<R, KTM_PICK_LINEAR, kWtPrefold>(jobs, n, s);
+    }
+    const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
+    if (a.pick == KTM_PICK_LINEAR)
+        return sq ? launch_batch_fmt<R, KTM_PICK_LINEAR, kWtSqrt>(jobs, n, s)
+                  : launch_batch_fmt<R, KTM_PICK_LINEAR, kWtTable>(jobs, n, s);
+    return sq ? launch_batch_fmt<R, KTM_PICK_TRUNCATE, kWtSqrt>(jobs, n, s)
+              : launch_batch_fmt<R, KTM_PICK_TRUNCATE, kWtTable>(jobs, n, s);
+}
+
+}  // namespace
+
+int launch_batch(const FastArgs* jobs, int njobs, cudaStream_t s)
+{
+    if (njobs <= 0) return KTM_OK;
+    const FastArgs& a = jobs[0];
+    for (int j = 0; j < njobs; j++) {
+        const FastArgs& b = jobs[j];
+        if (b.fmt != a.fmt || b.pick != a.pick || b.weightMode != a.weightMode ||
+            b.weightMethod != a.weightMethod)
+            return set_error(KTM_ERR_ARG, "batch: every job needs the same trace format, pick and weight");
+        const int esize = b.fmt == KTM_FMT_F32 ? 4 : 2;
+        if (b.g.ntr > 0 && (b.pitch < b.g.nt + 2 || ((size_t)b.pitch * esize) % 16 != 0 ||
+                            reinterpret_cast<uintptr_t>(b.traces) % 16 != 0))
+            return set_error(KTM_ERR_ARG, "batch: job %d traces are not a packed set", j);
+        if (b.g.nt >= (1 << 22)) return set_error(KTM_ERR_LIMIT, "batch: tracePts too large");
+    }
+    int R = a.tileRun > 0 ? a.tileRun / 32 : 0;
+    if (R == 0) {
+        int best = 16, bestWaste = 1 << 30;
+        for (int r : {16, 12, 8}) {
+            long long waste = 0;
+            for (int j = 0; j < njobs; j++) {
+                const int run = 32 * r, nz = jobs[j].g.nz;
+                waste += (long long)(((nz + run - 1) / run) * run - nz) * jobs[j].g.nx * jobs[j].g.ny;
+            }
+            if (waste < bestWaste) { bestWaste = (int)std::min<long long>(waste, 1 << 30); best = r; }
+        }
+        R = best;
+    }
+    switch (R) {
+        case 8: return launch_batch_r<8>(jobs, njobs, s);
+        case 12: return launch_batch_r<12>(jobs, njobs, s);
+        case 16: return launch_batch_r<16>(jobs, njobs, s);
+        default: return set_error(KTM_ERR_ARG, "batch: tileRun must be 256, 384 or 512");
+    }
 }
 
 }  // namespace ktm

@@ -67,6 +67,10 @@ struct FastArgs {
 // expects samples prefolded with sqrt(j*dt), truncating pick expects them not.
 int launch_fast(const FastArgs& a, cudaStream_t stream);
 
+// Persistent batched launch over many jobs (ktm_fast.cu): every job packed, same
+// format / pick / weight; images are overwritten.
+int launch_batch(const FastArgs* jobs, int njobs, cudaStream_t s);
+
 // ktm_adjoint.cu: demigration into the packed F32 layout [ntr][pitch]
 int launch_demigrate(const Geometry& g, const float* midX, const float* midY, const float* offX,
                      const float* offY, const float* vel, int velCube, const float* image,

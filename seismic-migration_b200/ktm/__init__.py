@@ -10,3 +10,4 @@ from .api import (  # noqa: F401
     grid, ktmMigrationCPU, ktmMigrationGPU, initThreeAxes, migrate, migrate_columns_f64, Job,
 )
 from .api import PackedTraces, packed_pitch, prepare  # noqa: F401,E402
+from .api import autotune, migrate_batch  # noqa: F401,E402

@@ -133,6 +133,10 @@ def lib() -> C.CDLL:
     L.ktmVrmsGradient.restype = C.c_int
     L.ktmLeastSquaresMigrate.argtypes = [C.POINTER(KtmLsm)]
     L.ktmLeastSquaresMigrate.restype = C.c_int
+    L.ktmMigrateBatch.argtypes = [C.POINTER(KtmJob), C.c_int, P]
+    L.ktmMigrateBatch.restype = C.c_int
+    L.ktmAutotune.argtypes = [C.POINTER(KtmJob), C.POINTER(C.c_int)]
+    L.ktmAutotune.restype = C.c_int
     L.ktmMigratePackedNoAlloc.argtypes = [C.POINTER(KtmJob)]
     L.ktmMigratePackedNoAlloc.restype = C.c_int
     L.ktmProbePeaks.argtypes = [P, P, P]

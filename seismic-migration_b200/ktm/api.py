@@ -256,6 +256,24 @@ def migrate(**kw):
     return Job(**kw).run()
 
 
+def migrate_batch(jobs, stream=None):
+    """Many jobs in one persistent launch (ktmMigrateBatch).  ``jobs`` is a list
+    of keyword dicts as for ``migrate`` (device memory, packed traces, images
+    given).  Returns the list of images."""
+    built = [Job(**kw) for kw in jobs]
+    arr = (KtmJob * len(built))(*[b.job for b in built])
+    check(lib().ktmMigrateBatch(arr, len(built), _stream_handle(stream)))
+    return [b.image for b in built]
+
+
+def autotune(**kw) -> int:
+    """Fastest tau-run length (tileRun) for this job's shapes (ktmAutotune)."""
+    job = Job(**kw)
+    out = C.c_int(0)
+    check(lib().ktmAutotune(C.byref(job.job), C.byref(out)))
+    return int(out.value)
+
+
 def migrate_columns_f64(*, columns=None, ncols=None, **kw):
     """FP64 device evaluation for a list of image columns -> torch float64 [ncols, Nz]."""
     import torch
