@@ -109,7 +109,10 @@ enum {
 enum {
     KTM_FMT_F32 = 0,
     KTM_FMT_F16 = 1,        /* IEEE half, multiplied by a per-trace FP32 scale */
-    KTM_FMT_BF16 = 2        /* bfloat16, multiplied by a per-trace FP32 scale */
+    KTM_FMT_BF16 = 2,       /* bfloat16, multiplied by a per-trace FP32 scale */
+    KTM_FMT_IBM32 = 3       /* IBM System/360 single precision words (inputData.bin,
+                               ioFunctions.c:4-40): raw traces only, converted on the
+                               device before filtering and packing */
 };
 
 /* Sample pick. */
@@ -128,7 +131,7 @@ typedef struct ktm_job {
     const float* offY;
     const void*  traces;                       /* [traceNo][traceStride] in traceFormat */
     const float* traceScale;                   /* [traceNo] multiplier (NULL: 1.0) */
-    int   traceFormat;                         /* KTM_FMT_* */
+    int   traceFormat;                         /* KTM_FMT_* (IBM32: raw traces only) */
     int   traceStride;                         /* samples between traces; 0 = tracePts */
     int   tracesPacked;                        /* 1: traces come from ktmPrepareTraces
                                                   (traceStride = its pitch, zero guard
@@ -193,7 +196,7 @@ typedef struct ktm_prep {
     int   traceNo, tracePts;
     int   inStride;            /* samples between input traces (0: tracePts) */
     float sampleRate;          /* s */
-    const float* in;           /* F32 [traceNo][inStride], device memory */
+    const float* in;           /* [traceNo][inStride] in inFormat, device memory */
     int   rho;                 /* KTM_RHO_*: the rho filter of ktmApplyRhoFilter.m:22-62
                                   (FFT length 2^ceil(log2 tracePts), omega = 2 pi k / dt
                                   with the script's scaling), applied per trace */
@@ -207,6 +210,8 @@ typedef struct ktm_prep {
     void* out;                 /* [traceNo][outPitch], device memory, 16-byte aligned */
     float* outScale;           /* [traceNo] per-trace scale, device memory */
     void* stream;              /* cudaStream_t */
+    int   inFormat;            /* KTM_FMT_F32 (0) or KTM_FMT_IBM32: IBM words converted as
+                                  ktmIBM32toIEEE does, in the same pass */
 } ktm_prep;
 
 /* Default pitch of a packed trace: tracePts + 2 rounded up to 16 bytes. */
@@ -303,6 +308,52 @@ int ktmMigratePackedNoAlloc(const ktm_job* job);
  * measure the error of the FP32 / FP16 / BF16 paths on images too large for a
  * CPU evaluation.  No counterpart in the reference. */
 int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, double* out);
+
+/* ------------------------------------------------------------------------ */
+/* The reference's data formats (host code, no device needed)               */
+/* ------------------------------------------------------------------------ */
+
+/* inp.txt: 12 space-separated numbers (ktmVisualizeOutputFile.m:22-48,
+ * ktmWriteTraceBlockConstOffset.m:154-167): tracePts, dt [s], traceNo,
+ * x start/step/points, y start/step/points, tau start/step/points. */
+typedef struct ktm_inp {
+    int   tracePts;
+    float sampleRate;          /* s */
+    int   traceNo;
+    struct imageGrid x, y, z;
+} ktm_inp;
+int ktmReadInp(const char* path, ktm_inp* inp);
+int ktmWriteInp(const char* path, const ktm_inp* inp);   /* same layout, "%f " per value */
+
+/* The survey of one data directory (loadInputData, ioFunctions.c:94-153):
+ * inputData.bin (traceNo x tracePts uint32 IBM-32 words when dataIsIBM, or
+ * float32 for the writers' impulse option), inputSrcX/Y.bin and inputRecX/Y.bin (float32
+ * [traceNo]), velModel.bin (float32 [Nz] or [Nx][Ny][Nz]).  Coordinates become
+ * midpoints and half offsets (ktmConvertXYtoOffMid.m:12) in FP64; with
+ * rebase = 1 they and the image axes are shifted by the survey origin (the
+ * smallest source/receiver x and y) before rounding to float.  Buffers are
+ * malloc'd; release them with ktmFreeSurvey. */
+typedef struct ktm_survey {
+    ktm_inp inp;
+    void* traces;              /* [traceNo][tracePts] 4-byte words in traceFormat */
+    int   traceFormat;         /* KTM_FMT_IBM32 or KTM_FMT_F32, as read: the words stay
+                                  unconverted for the device (ktm_job.traceFormat) */
+    float *midX, *midY, *offX, *offY;
+    float* velocity;
+    int   velocityCube;
+    double originX, originY;   /* subtracted when rebased */
+} ktm_survey;
+int ktmLoadSurvey(const char* dir, int dataIsIBM, int rebase, ktm_survey* out);
+void ktmFreeSurvey(ktm_survey* s);
+/* outputData.bin: float32 [Nx][Ny][Nz], tau fastest (ktmVisualizeOutputFile.m:16-28). */
+int ktmWriteImage(const char* path, const float* image, size_t count);
+
+/* ioFunctions.c:4-40 (same name and arguments): IBM-32 words to IEEE float,
+ * sign * (fraction / 0xFFFFFF) * 16^(exponent - 64), on the current device
+ * (host buffers, synchronous).  Bit-identical to the reference. */
+void ktmIBM32toIEEE(unsigned int* input, float* output, int n);
+/* The same conversion on device buffers, asynchronous on `stream`. */
+int ktmIBM32toIEEEDevice(const unsigned int* input, float* output, size_t n, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic data and measurement                                           */

@@ -59,7 +59,7 @@ int make_geometry(const ktm_job* j, Geometry* g)
     return KTM_OK;
 }
 
-size_t fmt_bytes(int fmt) { return fmt == KTM_FMT_F32 ? 4 : 2; }
+size_t fmt_bytes(int fmt) { return (fmt == KTM_FMT_F32 || fmt == KTM_FMT_IBM32) ? 4 : 2; }
 
 // Device copies of a host-memory job (freed in the destructor, stream-ordered).
 struct Staged {
@@ -97,13 +97,25 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
                const float* vel, float* image, cudaStream_t s)
 {
     if (j->mode == KTM_MODE_REFERENCE) {
-        if (j->traceFormat != KTM_FMT_F32 || j->pick != KTM_PICK_TRUNCATE || j->velocityCube ||
-            j->aperture > 0.0f || j->tracesPrefolded || scale)
+        const bool ibm = j->traceFormat == KTM_FMT_IBM32;
+        if ((j->traceFormat != KTM_FMT_F32 && !ibm) || j->pick != KTM_PICK_TRUNCATE ||
+            j->velocityCube || j->aperture > 0.0f || j->tracesPrefolded || scale)
             return set_error(KTM_ERR_ARG,
-                             "reference mode takes F32 traces, truncating pick, no aperture, "
-                             "no scale and a 1-D velocity (psktmCPU.c semantics)");
-        return launch_reference(g, midX, midY, offX, offY, static_cast<const float*>(traces), vel,
-                                image, j->accumulate, j->tileRun, s);
+                             "reference mode takes F32 or IBM-32 traces, truncating pick, no "
+                             "aperture, no scale and a 1-D velocity (psktmCPU.c semantics)");
+        if (!ibm)
+            return launch_reference(g, midX, midY, offX, offY, static_cast<const float*>(traces),
+                                    vel, image, j->accumulate, j->tileRun, s);
+        // IBM words: convert on the device (ioFunctions.c:4-40), then migrate
+        const size_t n = (size_t)g.ntr * g.stride;
+        void* conv = nullptr;
+        if (n) KTM_CUDA_TRY(cudaMallocAsync(&conv, n * 4, s));
+        int rc = ibm_to_ieee(static_cast<const uint32_t*>(traces), static_cast<float*>(conv), n, s);
+        if (!rc)
+            rc = launch_reference(g, midX, midY, offX, offY, static_cast<const float*>(conv), vel,
+                                  image, j->accumulate, j->tileRun, s);
+        if (conv) cudaFreeAsync(conv, s);
+        return rc;
     }
     if (j->mode == KTM_MODE_FAST) {
         FastArgs a;
@@ -121,6 +133,8 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         a.weightMethod = j->weightMethod;
         const int wantPrefold = 0;
         if (j->tracesPacked) {
+            if (j->traceFormat == KTM_FMT_IBM32)
+                return set_error(KTM_ERR_ARG, "packed traces cannot be IBM-32");
             a.traces = traces; a.scale = scale; a.fmt = j->traceFormat; a.pitch = g.stride;
             if (!scale) return set_error(KTM_ERR_ARG, "packed traces need traceScale");
             return launch_fast(a, s);
@@ -134,7 +148,7 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         const float* src32 = in;
         void* widened = nullptr;
         int rc = KTM_OK;
-        if (j->traceFormat != KTM_FMT_F32) {
+        if (j->traceFormat == KTM_FMT_F16 || j->traceFormat == KTM_FMT_BF16) {
             // half-precision input: widen (times its scale) to F32 first
             rc = widen_traces(traces, j->traceFormat, scale, g.ntr, g.nt, g.stride, &widened, s);
             if (rc) return rc;
@@ -152,6 +166,8 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
             p.traceNo = g.ntr; p.tracePts = g.nt;
             p.inStride = widened ? g.nt : g.stride;
             p.sampleRate = g.dt; p.in = src32; p.prefold = wantPrefold; p.rho = j->rho;
+            // IBM words are converted inside the preparation pass
+            p.inFormat = j->traceFormat == KTM_FMT_IBM32 ? KTM_FMT_IBM32 : KTM_FMT_F32;
             p.outFormat = j->packFormat; p.outPitch = pitch; p.out = packed; p.outScale = pscale;
             p.stream = s;
             rc = prepare_traces(&p);
@@ -172,8 +188,10 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
 int check_job(const ktm_job* j)
 {
     if (!j) return set_error(KTM_ERR_ARG, "NULL job");
-    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_BF16)
+    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_IBM32)
         return set_error(KTM_ERR_ARG, "bad traceFormat %d", j->traceFormat);
+    if (j->traceFormat == KTM_FMT_IBM32 && (j->traceScale || j->tracesPacked))
+        return set_error(KTM_ERR_ARG, "IBM-32 traces are raw: no traceScale, not packed");
     if (j->pick != KTM_PICK_TRUNCATE && j->pick != KTM_PICK_LINEAR)
         return set_error(KTM_ERR_ARG, "bad pick %d", j->pick);
     const bool needTraces = j->config.traceNo > 0;
@@ -248,6 +266,10 @@ void dropin(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* 
 }  // namespace ktm
 
 extern "C" {
+
+// status hooks of the host-side file I/O (ktm_io.c)
+int ktm_io_error(int code, const char* msg) { return ktm::set_error(code, "%s", msg); }
+int ktm_io_ok(void) { return ktm::set_ok(); }
 
 int ktmGetLastError(void) { return ktm::tl_code; }
 const char* ktmGetLastErrorMessage(void) { return ktm::tl_msg; }
@@ -326,6 +348,9 @@ int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, doub
     if (!job->deviceMemory)
         return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64 takes device memory");
     if (ncols < 0 || (!out && ncols > 0)) return ktm::set_error(KTM_ERR_ARG, "bad column list");
+    if (job->traceFormat == KTM_FMT_IBM32)
+        return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64: convert IBM-32 traces first "
+                                           "(ktmIBM32toIEEEDevice)");
     ktm::Geometry g;
     rc = ktm::make_geometry(job, &g);
     if (rc) return rc;

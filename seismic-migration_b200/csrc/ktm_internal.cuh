@@ -88,6 +88,9 @@ int prepare_traces(const ktm_prep* p);
 int widen_traces(const void* in, int fmt, const float* scale, int ntr, int nt, int stride,
                  void** out, cudaStream_t s);
 
+// ktm_ibm.cu: IBM-32 words -> IEEE float, bit-identical to ktmIBM32toIEEE.
+int ibm_to_ieee(const uint32_t* in, float* out, size_t n, cudaStream_t s);
+
 // FP64 device reference (ktm_fast.cu): out[q][nz] for image columns cols[q]
 // (cols == NULL: columns 0..ncols-1).
 int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* out,

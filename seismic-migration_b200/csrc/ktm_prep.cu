@@ -15,6 +15,7 @@
 //   out[k][j] = Q(x'_j / s_k), x'_j = filtered x_j (times sqrt(j dt) when
 //   prefold), 0 < j < tracePts; out[k][0] = out[k][j >= tracePts] = 0.
 //   s_k = max|x'| (BF16), max|x'| / 32768 (F16), 1 (F32).
+#include "ktm_ibm.cuh"
 #include "ktm_internal.cuh"
 
 #include <cuda_bf16.h>
@@ -103,11 +104,19 @@ struct PrepArgs {
     int ntr, nt, inStride, pitch;
     float dt;
     const float* in;
+    int ibm;                 // 1: in holds IBM-32 words
     int rho, scriptOrder, prefold;
     void* out;
     float* scale;
     int M, logM;
 };
+
+// input sample n of the trace at p (IBM words converted as ktmIBM32toIEEE does)
+__device__ __forceinline__ float load_in(const float* p, int n, int ibm)
+{
+    if (ibm) return dev::ibm32_to_f32(reinterpret_cast<const uint32_t*>(p)[n]);
+    return p[n];
+}
 
 template <int FMT>
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a)
@@ -131,8 +140,8 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a)
         }
         // bit-reversed load of z = x + i y, zero padded to M (fft(trace', M), :37)
         for (int n = threadIdx.x; n < M; n += blockDim.x) {
-            float xr = n < a.nt ? x[n] : 0.0f;
-            float yi = (two && n < a.nt) ? y[n] : 0.0f;
+            float xr = n < a.nt ? load_in(x, n, a.ibm) : 0.0f;
+            float yi = (two && n < a.nt) ? load_in(y, n, a.ibm) : 0.0f;
             z[bitrev((unsigned)n, a.logM)] = make_float2(xr, yi);
         }
         __syncthreads();
@@ -162,7 +171,7 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(PrepArgs a)
         __syncthreads();
     } else {
         for (int n = threadIdx.x; n < a.nt; n += blockDim.x)
-            z[n] = make_float2(x[n], two ? y[n] : 0.0f);
+            z[n] = make_float2(load_in(x, n, a.ibm), two ? load_in(y, n, a.ibm) : 0.0f);
         __syncthreads();
     }
 
@@ -249,6 +258,8 @@ int prepare_traces(const ktm_prep* p)
     if (p->outFormat < KTM_FMT_F32 || p->outFormat > KTM_FMT_BF16)
         return set_error(KTM_ERR_ARG, "bad outFormat %d", p->outFormat);
     if (p->rho < KTM_RHO_NONE || p->rho > KTM_RHO_3D) return set_error(KTM_ERR_ARG, "bad rho %d", p->rho);
+    if (p->inFormat != KTM_FMT_F32 && p->inFormat != KTM_FMT_IBM32)
+        return set_error(KTM_ERR_ARG, "bad inFormat %d (F32 or IBM32)", p->inFormat);
     if (!(p->sampleRate > 0.0f)) return set_error(KTM_ERR_ARG, "sampleRate must be > 0");
     if (p->traceNo == 0) return KTM_OK;
     if (!p->in || !p->out || !p->outScale) return set_error(KTM_ERR_ARG, "NULL buffer");
@@ -262,7 +273,7 @@ int prepare_traces(const ktm_prep* p)
         return set_error(KTM_ERR_ARG, "outPitch must be >= tracePts + 2 and a multiple of 16 bytes");
     if (reinterpret_cast<uintptr_t>(p->out) % 16 != 0)
         return set_error(KTM_ERR_ARG, "out must be 16-byte aligned");
-    a.dt = p->sampleRate; a.in = p->in; a.rho = p->rho; a.scriptOrder = p->rhoScriptOrder;
+    a.dt = p->sampleRate; a.in = p->in; a.ibm = p->inFormat == KTM_FMT_IBM32; a.rho = p->rho; a.scriptOrder = p->rhoScriptOrder;
     a.prefold = p->prefold; a.out = p->out; a.scale = p->outScale;
     a.M = 1; a.logM = 0;
     while (a.M < a.nt) { a.M <<= 1; a.logM++; }

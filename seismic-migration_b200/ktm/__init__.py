@@ -11,3 +11,4 @@ from .api import (  # noqa: F401
 )
 from .api import PackedTraces, packed_pitch, prepare  # noqa: F401,E402
 from .api import autotune, migrate_batch  # noqa: F401,E402
+from . import io  # noqa: F401,E402

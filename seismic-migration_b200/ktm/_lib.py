@@ -23,7 +23,7 @@ KTM_ERR_TIMEOUT = 6
 KTM_ERR_NODEVICE = 7
 
 KTM_MODE_REFERENCE, KTM_MODE_FAST, KTM_MODE_F64 = 0, 1, 2
-KTM_FMT_F32, KTM_FMT_F16, KTM_FMT_BF16 = 0, 1, 2
+KTM_FMT_F32, KTM_FMT_F16, KTM_FMT_BF16, KTM_FMT_IBM32 = 0, 1, 2, 3
 KTM_PICK_TRUNCATE, KTM_PICK_LINEAR = 0, 1
 KTM_RHO_NONE, KTM_RHO_2D, KTM_RHO_25D, KTM_RHO_3D = 0, 1, 2, 3
 
@@ -78,7 +78,7 @@ class KtmPrep(C.Structure):
         ("traceNo", C.c_int), ("tracePts", C.c_int), ("inStride", C.c_int),
         ("sampleRate", C.c_float), ("in_", P), ("rho", C.c_int), ("rhoScriptOrder", C.c_int),
         ("prefold", C.c_int), ("outFormat", C.c_int), ("outPitch", C.c_int), ("out", P),
-        ("outScale", P), ("stream", P),
+        ("outScale", P), ("stream", P), ("inFormat", C.c_int),
     ]
 
 
@@ -89,6 +89,20 @@ class KtmLsm(C.Structure):
         ("iterations", C.c_int), ("useGraph", C.c_int), ("residualNorms", P),
         ("gradientNorms", P),
     ]
+
+
+class KtmInp(C.Structure):
+    """ktm_inp (include/ktm.h): the 12 numbers of inp.txt."""
+    _fields_ = [("tracePts", C.c_int), ("sampleRate", C.c_float), ("traceNo", C.c_int),
+                ("x", ImageGrid), ("y", ImageGrid), ("z", ImageGrid)]
+
+
+class KtmSurvey(C.Structure):
+    """ktm_survey (include/ktm.h): one data directory read by ktmLoadSurvey."""
+    _fields_ = [("inp", KtmInp), ("traces", P), ("traceFormat", C.c_int),
+                ("midX", P), ("midY", P), ("offX", P), ("offY", P),
+                ("velocity", P), ("velocityCube", C.c_int),
+                ("originX", C.c_double), ("originY", C.c_double)]
 
 
 _lib = None
@@ -144,6 +158,20 @@ def lib() -> C.CDLL:
     L.ktmSynthesizeTraces.argtypes = [C.c_int, C.c_int, C.c_float, P, P, P, P, C.c_int, P,
                                       C.c_double, C.c_double, C.c_ulonglong, C.c_int, P, P]
     L.ktmSynthesizeTraces.restype = C.c_int
+    L.ktmReadInp.argtypes = [C.c_char_p, C.POINTER(KtmInp)]
+    L.ktmReadInp.restype = C.c_int
+    L.ktmWriteInp.argtypes = [C.c_char_p, C.POINTER(KtmInp)]
+    L.ktmWriteInp.restype = C.c_int
+    L.ktmLoadSurvey.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(KtmSurvey)]
+    L.ktmLoadSurvey.restype = C.c_int
+    L.ktmFreeSurvey.argtypes = [C.POINTER(KtmSurvey)]
+    L.ktmFreeSurvey.restype = None
+    L.ktmWriteImage.argtypes = [C.c_char_p, P, C.c_size_t]
+    L.ktmWriteImage.restype = C.c_int
+    L.ktmIBM32toIEEE.argtypes = [P, P, C.c_int]
+    L.ktmIBM32toIEEE.restype = None
+    L.ktmIBM32toIEEEDevice.argtypes = [P, P, C.c_size_t, P]
+    L.ktmIBM32toIEEEDevice.restype = C.c_int
     _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "

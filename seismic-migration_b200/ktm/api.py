@@ -17,7 +17,8 @@ from ._lib import ImageGrid, JobParams, KtmError, KtmJob, check, lib
 
 _PICK = {"truncate": _lib.KTM_PICK_TRUNCATE, "linear": _lib.KTM_PICK_LINEAR}
 _MODE = {"reference": _lib.KTM_MODE_REFERENCE, "fast": _lib.KTM_MODE_FAST}
-_FMT = {"f32": _lib.KTM_FMT_F32, "f16": _lib.KTM_FMT_F16, "bf16": _lib.KTM_FMT_BF16}
+_FMT = {"f32": _lib.KTM_FMT_F32, "f16": _lib.KTM_FMT_F16, "bf16": _lib.KTM_FMT_BF16,
+        "ibm32": _lib.KTM_FMT_IBM32}
 
 
 def grid(n: int, step: float, start: float = 0.0) -> ImageGrid:
@@ -145,10 +146,13 @@ def packed_pitch(nt: int, fmt: str = "bf16") -> int:
 def prepare(traces, dt: float, *, fmt: str = "bf16", rho=0, prefold: bool = True,
             script_order: bool = False, stream=None, out=None, out_scale=None) -> PackedTraces:
     """Rho filter (ktmApplyRhoFilter.m option 1/2/3), sqrt(t) weight fold,
-    per-trace scale and quantisation on the device (ktmPrepareTraces)."""
+    per-trace scale and quantisation on the device (ktmPrepareTraces).  An
+    int32/uint32 tensor holds IBM-32 words, converted in the same pass."""
     import torch
-    if not (_is_torch(traces) and traces.is_cuda and traces.dtype == torch.float32):
-        raise ValueError("prepare takes a CUDA float32 tensor [traceNo, tracePts]")
+    ibm = _is_torch(traces) and traces.dtype in (torch.int32, torch.uint32)
+    if not (_is_torch(traces) and traces.is_cuda and (traces.dtype == torch.float32 or ibm)):
+        raise ValueError("prepare takes a CUDA float32 (or IBM-32 int32) tensor "
+                         "[traceNo, tracePts]")
     traces = traces.contiguous()
     ntr, nt = traces.shape
     pitch = packed_pitch(nt, fmt)
@@ -168,6 +172,7 @@ def prepare(traces, dt: float, *, fmt: str = "bf16", rho=0, prefold: bool = True
     p.out = out.data_ptr()
     p.outScale = out_scale.data_ptr()
     p.stream = _stream_handle(stream)
+    p.inFormat = _lib.KTM_FMT_IBM32 if ibm else _lib.KTM_FMT_F32
     check(lib().ktmPrepareTraces(C.byref(p)))
     return PackedTraces(out, out_scale, nt, fmt, prefold, p.rho)
 
@@ -197,7 +202,8 @@ class Job:
             ntr = traces.shape[0]
             nt = packed.nt if packed is not None else traces.shape[1]
             if fmt is None:
-                fmt = {torch.float32: "f32", torch.float16: "f16", torch.bfloat16: "bf16"}[traces.dtype]
+                fmt = {torch.float32: "f32", torch.float16: "f16", torch.bfloat16: "bf16",
+                       torch.int32: "ibm32", torch.uint32: "ibm32"}[traces.dtype]
             if image is None:
                 image = torch.empty((nx, ny, nz), device=traces.device, dtype=torch.float32)
             for a in (midX, midY, offX, offY, velocity, image, scale):
@@ -206,8 +212,8 @@ class Job:
         else:
             traces = np.ascontiguousarray(traces)
             if fmt is None:
-                fmt = {np.dtype(np.float32): "f32", np.dtype(np.float16): "f16"}.get(
-                    traces.dtype, "f32")
+                fmt = {np.dtype(np.float32): "f32", np.dtype(np.float16): "f16",
+                       np.dtype(np.uint32): "ibm32"}.get(traces.dtype, "f32")
                 if fmt == "f32":
                     traces = _f32(traces)
             midX, midY, offX, offY, velocity = map(_f32, (midX, midY, offX, offY, velocity))

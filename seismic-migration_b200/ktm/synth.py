@@ -254,3 +254,33 @@ def synthesize(sv: Survey, k0: int = 0, k1: int | None = None, noise: bool = Tru
     if noise and sv.noise > 0:
         out += sv.noise * hash_noise(sv.seed, sv.meta.get("trace_offset", 0) + k0, n, sv.nt)
     return out.astype(np.float32)
+
+
+def encode_ibm32(x) -> np.ndarray:
+    """IEEE -> IBM System/360 single precision words (sign, base-16 exponent
+    biased by 64, 24-bit fraction in [1/16, 1)), rounding the fraction to
+    nearest: synthetic IBM data of the kind inputData.bin holds.  Values beyond
+    the IBM range clamp to its largest / smallest exponent."""
+    a64 = np.asarray(x, np.float64)
+    out = np.zeros(a64.shape, np.uint32)
+    a = np.abs(a64)
+    nz = a > 0
+    if not nz.any():
+        return out
+    v = a[nz]
+    e = np.floor(np.log2(v) / 4.0).astype(np.int64) + 1          # v = f 16^e, f in [1/16, 1)
+    f = v / np.power(16.0, e.astype(np.float64))
+    lo = f < 1.0 / 16.0
+    e[lo] -= 1
+    f[lo] *= 16.0
+    hi = f >= 1.0
+    e[hi] += 1
+    f[hi] /= 16.0
+    frac = np.rint(f * float(1 << 24)).astype(np.int64)
+    up = frac >= (1 << 24)                                           # rounded up to 1.0
+    frac[up] = 1 << 20
+    e[up] += 1
+    e = np.clip(e + 64, 0, 127)
+    sign = (a64[nz] < 0).astype(np.int64) << 31
+    out[nz] = (sign | (e << 24) | frac).astype(np.uint32)
+    return out
