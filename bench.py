@@ -60,14 +60,18 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--skip-error", action="store_true", help="skip the FP64 error check")
-    ap.add_argument("--prefold", action="store_true",
-                    help="fold sqrt(t) into the packed samples (faster, less accurate)")
     ap.add_argument("--config", default="3d", choices=["3d", "batch"],
                     help="3d: the headline workload; batch: 64 target-oriented jobs in one "
                          "persistent launch")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--lsm-jobs", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--tile-run", type=int, default=0,
+                    help="tau samples per warp run: 256, 384 or 512 (0: chosen by Nz)")
+    ap.add_argument("--weight", default="prefold", choices=["prefold", "table", "sqrt"],
+                    help="sqrt(t) of the weight: folded into the packed samples as sqrt(j dt) "
+                         "(default), from the kernel's interpolated sqrt(j dt) table, or one "
+                         "sqrt.approx per pair")
     return ap.parse_args()
 
 
@@ -345,7 +349,8 @@ def main():
         k0, k1 = bounds[i % nb]
         n = k1 - k0
         with torch.cuda.stream(stream):
-            p = ktm.prepare(raw[k0:k1], sv.dt, fmt=a.fmt, rho=sv.rho_opt, prefold=a.prefold,
+            p = ktm.prepare(raw[k0:k1], sv.dt, fmt=a.fmt, rho=sv.rho_opt,
+                            prefold=a.weight == "prefold",
                             stream=stream, out=pbuf[:n], out_scale=pscale[:n])
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -354,7 +359,8 @@ def main():
                         midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
                         offY=coords[3][k0:k1], traces=p, velocity=vel, image=image,
                         pick="linear", aperture=sv.aperture, accumulate=(i > 0), stream=stream,
-                        pairs_counter=counter if count else None)
+                        pairs_counter=counter if count else None, weight=a.weight,
+                        tile_run=a.tile_run)
             e1.record(stream)
         return e0, e1, n
 
@@ -461,7 +467,7 @@ def main():
                   midX=h_c[0].numpy(), midY=h_c[1].numpy(), offX=h_c[2].numpy(),
                   offY=h_c[3].numpy(), traces=h_tr.numpy(), velocity=h_v.numpy(),
                   image=h_img.numpy(), pick="linear", aperture=sv.aperture, rho=sv.rho_opt,
-                  pack_format=a.fmt, stream=stream)
+                  pack_format=a.fmt, weight=a.weight, stream=stream)
         ktm.migrate(**hk)   # warm-up
         he0, he1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
@@ -504,8 +510,9 @@ def main():
             "config": {"workload": WORKLOAD, "traces": sv.ntr, "image": [nx, ny, nz],
                        "batch_traces": bsz, "trace_format": a.fmt, "rho": "3D (i*omega)",
                        "pick": "linear", "aperture_m": sv.aperture,
-                       "weight": ("sqrt(j dt) folded into the samples" if a.prefold else
-                                  "sqrt(t) from the interpolated sqrt(j dt) table"),
+                       "weight": {"prefold": "sqrt(j dt) folded into the packed samples",
+                                  "table": "sqrt(t) from the interpolated sqrt(j dt) table",
+                                  "sqrt": "sqrt(t) by sqrt.approx per pair"}[a.weight],
                        "l2": "each step reads a new 375 MB batch (> 126 MB L2)",
                        "parallelism": f"{world} GPU(s), one image tile per GPU, no collective"},
             "plain_fp32": {"value": plain_rate, "unit": UNIT,

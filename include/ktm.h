@@ -164,7 +164,14 @@ typedef struct ktm_job {
 enum {
     KTM_WEIGHT_TABLE = 0,   /* sqrt(j*dt) table interpolated at t/dt (relative error
                                ~1/(32 j^2)) -- two special-function ops per pair */
-    KTM_WEIGHT_SQRT = 1     /* sqrt.approx per pair -- three special-function ops */
+    KTM_WEIGHT_SQRT = 1,    /* sqrt.approx per pair -- three special-function ops */
+    KTM_WEIGHT_PREFOLD = 2  /* ktmMigrate prepares raw traces with sqrt(j*dt) folded into
+                               the samples (ktm_prep.prefold = 1): no weight work per pair.
+                               Interpolating the product instead of the factors differs
+                               from the reference weight by f(1-f) dg dd per pick (about
+                               1e-4 relative L2 on deep images, up to ~6e-4 on shallow
+                               ones); linear pick only.  Packed traces must have been
+                               prepared with prefold = 1 (tracesPrefolded). */
 };
 
 /* Zero-initialise a job and fill in defaults (mode FAST, pick LINEAR, F32,

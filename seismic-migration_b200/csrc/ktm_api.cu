@@ -126,12 +126,18 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         a.pick = j->pick; a.aperture = j->aperture;
         a.tileRun = j->tileRun; a.tileCols = j->tileCols;
         a.pairsEvaluated = j->pairsEvaluated;
-        // weight sqrt(t): from the kernel's table (0) or folded into the packed samples (2)
+        // weight sqrt(t): from the kernel's table / sqrt (0) or folded into the packed samples (2)
         a.weightMode = (j->tracesPacked && j->tracesPrefolded) ? 2 : 0;
-        if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
+        if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT &&
+            j->weightMethod != KTM_WEIGHT_PREFOLD)
             return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
-        a.weightMethod = j->weightMethod;
-        const int wantPrefold = 0;
+        const int wantPrefold = j->weightMethod == KTM_WEIGHT_PREFOLD;
+        if (wantPrefold && j->pick != KTM_PICK_LINEAR)
+            return set_error(KTM_ERR_ARG, "KTM_WEIGHT_PREFOLD takes the linear pick");
+        if (wantPrefold && j->tracesPacked && !j->tracesPrefolded)
+            return set_error(KTM_ERR_ARG, "KTM_WEIGHT_PREFOLD with packed traces: prepare them "
+                                          "with prefold = 1");
+        a.weightMethod = wantPrefold ? KTM_WEIGHT_TABLE : j->weightMethod;
         if (j->tracesPacked) {
             if (j->traceFormat == KTM_FMT_IBM32)
                 return set_error(KTM_ERR_ARG, "packed traces cannot be IBM-32");
@@ -173,6 +179,7 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
             rc = prepare_traces(&p);
             if (!rc) {
                 a.traces = packed; a.scale = pscale; a.fmt = j->packFormat; a.pitch = pitch;
+                a.weightMode = wantPrefold ? 2 : 0;
                 rc = launch_fast(a, s);
             }
         }
@@ -435,7 +442,8 @@ int packed_args(const ktm_job* j, FastArgs* a)
                                       "and packed traces");
     int rc = check_job(j);
     if (rc) return rc;
-    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
+    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT &&
+        !(j->weightMethod == KTM_WEIGHT_PREFOLD && j->tracesPrefolded))
         return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
     std::memset(a, 0, sizeof(*a));
     rc = make_geometry(j, &a->g);
@@ -444,7 +452,7 @@ int packed_args(const ktm_job* j, FastArgs* a)
     a->midX = j->midX; a->midY = j->midY; a->offX = j->offX; a->offY = j->offY;
     a->traces = j->traces; a->scale = j->traceScale; a->fmt = j->traceFormat; a->pitch = a->g.stride;
     a->weightMode = j->tracesPrefolded ? 2 : 0;
-    a->weightMethod = j->weightMethod;
+    a->weightMethod = j->weightMethod == KTM_WEIGHT_PREFOLD ? KTM_WEIGHT_TABLE : j->weightMethod;
     a->vel = j->velocity; a->velCube = j->velocityCube;
     a->image = j->image; a->accumulate = j->accumulate;
     a->pick = j->pick; a->aperture = j->aperture;

@@ -373,8 +373,9 @@ __global__ void reduce_slices(float* __restrict__ out, const float* __restrict__
     }
 }
 
+// One grid launch over all of a's traces.
 template <int R, int PICK, int FMT, int PRE, int GRAD>
-int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
+int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const Geometry& g = a.g;
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
@@ -424,6 +425,35 @@ int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
     }
     if (partial && partial != a.scratch) cudaFreeAsync(partial, stream);
     if (e != cudaSuccess) return set_error(KTM_ERR_CUDA, "fast kernel launch: %s", cudaGetErrorString(e));
+    return KTM_OK;
+}
+
+// Packed trace bytes per launch.  Every CTA streams all traces of its launch
+// and CTAs start at different times, so the traces of one launch should stay
+// resident in L2 (126 MB) while they are read: a trace set larger than this
+// goes in blocks, one launch each, the later ones accumulating.
+constexpr size_t kTraceBlockBytes = 40u << 20;
+
+template <int R, int PICK, int FMT, int PRE, int GRAD>
+int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
+{
+    const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
+    const size_t rowBytes = (size_t)a.pitch * esize;
+    const int block = (int)std::max<size_t>(1024, kTraceBlockBytes / rowBytes);
+    if (a.g.ntr <= block) return launch_block<R, PICK, FMT, PRE, GRAD>(a, stream, smCount);
+    // balanced blocks of at most `block` traces
+    const int nblk = (a.g.ntr + block - 1) / block;
+    const int per = (a.g.ntr + nblk - 1) / nblk;
+    for (int kb = 0; kb < a.g.ntr; kb += per) {
+        FastArgs b = a;
+        b.g.ntr = std::min(per, a.g.ntr - kb);
+        b.midX = a.midX + kb; b.midY = a.midY + kb; b.offX = a.offX + kb; b.offY = a.offY + kb;
+        b.traces = static_cast<const unsigned char*>(a.traces) + (size_t)kb * rowBytes;
+        b.scale = a.scale ? a.scale + kb : nullptr;
+        b.accumulate = a.accumulate || kb > 0;
+        const int rc = launch_block<R, PICK, FMT, PRE, GRAD>(b, stream, smCount);
+        if (rc) return rc;
+    }
     return KTM_OK;
 }
 

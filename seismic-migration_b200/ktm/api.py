@@ -249,7 +249,7 @@ class Job:
         j.pairsEvaluated = _ptr(pairs_counter)
         j.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
         j.packFormat = _FMT[pack_format]
-        j.weightMethod = {"table": 0, "sqrt": 1}[weight]
+        j.weightMethod = {"table": 0, "sqrt": 1, "prefold": 2}[weight]
         self.job = j
 
     def run(self):

@@ -341,3 +341,49 @@ def test_fast_sqrt_weight_matches_reference_weight(cuda, ktm_lib, pick):
     img = fast(cuda, case, pick=pick, weight="sqrt")
     ref = oracle.migrate_f64(*case, pick=1 if pick == "linear" else 0, prefold=0)
     assert rel_l2(img, ref) < (2e-5 if pick == "linear" else TRUNC_GATE)
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+def test_prefold_weight_on_raw_traces(cuda, ktm_lib, fmt):
+    """KTM_WEIGHT_PREFOLD on raw traces: ktmMigrate prepares them with the
+    sqrt(j dt) fold; same result as packing with prefold=1 and migrating."""
+    import ktm
+    case = random_case(16, ntr=170, nz=280, data="ricker")
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    kw = dict(imageX=gx, imageY=gy, imageZ=gz, dt=dt, midX=_t(mx, cuda), midY=_t(my, cuda),
+              offX=_t(ox, cuda), offY=_t(oy, cuda), velocity=_t(vel, cuda), pick="linear")
+    a = ktm.migrate(traces=_t(tr, cuda), weight="prefold", pack_format=fmt, **kw).cpu().numpy()
+    p = ktm.prepare(_t(tr, cuda), dt, fmt=fmt, prefold=True)
+    b = ktm.migrate(traces=p, **kw).cpu().numpy()
+    assert np.array_equal(a, b)
+    ref0 = oracle.migrate_f64(*case, pick=1, prefold=0)
+    assert rel_l2(a, ref0) < GATE[fmt]
+    with pytest.raises(ktm.KtmError):
+        ktm.migrate(traces=_t(tr, cuda), weight="prefold", **dict(kw, pick="truncate"))
+    unfolded = ktm.prepare(_t(tr, cuda), dt, fmt=fmt, prefold=False)
+    with pytest.raises(ktm.KtmError):
+        ktm.migrate(traces=unfolded, weight="prefold", **kw)
+
+
+def test_fast_trace_blocks_for_large_sets(cuda, ktm_lib):
+    """A packed set larger than the per-launch trace block (40 MB) runs as
+    several launches accumulating into the image: same result as the oracle."""
+    import ktm
+    rng = np.random.default_rng(17)
+    ntr, nt = 24000, 1000                     # f16 rows of 2016 B: 48 MB, two blocks
+    gx, gy, gz = oracle.grid(3, 40.0, -40.0), oracle.grid(2, 40.0, 0.0), oracle.grid(120, 0.004, 0.0)
+    mid = rng.uniform(-200, 200, (ntr, 2)).astype(np.float32)
+    off = rng.uniform(-200, 200, (ntr, 2)).astype(np.float32)
+    tr = band_limited(rng, ntr, nt, 0.004)
+    vel = np.linspace(1500.0, 2500.0, 120).astype(np.float32)
+    p = ktm.prepare(_t(tr, cuda), 0.004, fmt="f16", prefold=True)
+    assert p.data.numel() * 2 > (40 << 20)
+    c = __import__("torch").zeros(1, device=cuda, dtype=__import__("torch").int64)
+    img = ktm.migrate(imageX=gx, imageY=gy, imageZ=gz, dt=0.004, midX=_t(mid[:, 0], cuda),
+                      midY=_t(mid[:, 1], cuda), offX=_t(off[:, 0], cuda), offY=_t(off[:, 1], cuda),
+                      traces=p, velocity=_t(vel, cuda), pick="linear", pairs_counter=c).cpu().numpy()
+    q = (p.data.float() * p.scale[:, None]).cpu().numpy()
+    same = oracle.migrate_f64(gx, gy, gz, 0.004, mid[:, 0], mid[:, 1], off[:, 0], off[:, 1],
+                              np.ascontiguousarray(q[:, :nt]), vel, pick=1, prefold=2)
+    assert rel_l2(img, same) < 2e-5
+    assert 0 < int(c.item()) <= ntr * 3 * 2 * 120
