@@ -404,6 +404,20 @@ def main():
     # evaluated pairs (after aperture / end-of-trace culling), counted by the kernel
     evaluated = int(counter.item())
     sfu_rate = evaluated * 2 / (kernel_ms * 1e-3)      # two sqrt.approx per evaluated pair
+    # in-aperture pairs of the timed batches, counted independently of the kernel
+    # (|mid - x| <= aperture over all image columns, in FP64; times Nz)
+    in_aperture = 0
+    cx = (sv.imageX.imageStart + sv.imageX.imageStep *
+          torch.arange(nx, device=dev, dtype=torch.float64)).repeat_interleave(ny)
+    cy = (sv.imageY.imageStart + sv.imageY.imageStep *
+          torch.arange(ny, device=dev, dtype=torch.float64)).repeat(nx)
+    for i in range(a.steps):
+        k0, k1 = bounds[i % nb]
+        for j0 in range(k0, k1, 4096):
+            j1 = min(k1, j0 + 4096)
+            dx = coords[0][j0:j1, None].double() - cx[None, :]
+            dy = coords[1][j0:j1, None].double() - cy[None, :]
+            in_aperture += int(((dx * dx + dy * dy) <= sv.aperture ** 2).sum().item()) * nz
 
     # ---- accuracy: one batch, fresh image, vs FP64 device evaluation (rho-filtered
     # FP32 input, weight |tau| sqrt(t) per pair) on sampled columns
@@ -490,18 +504,31 @@ def main():
         r, cores, kind, sample = cpu_reference_rate(sub, a.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
+    # DRAM bytes of one step from the ncu capture summarised in profiles/ (one step of
+    # the same workload), scaled to this batch by its traces
     traffic = None
     tf = os.path.join(ROOT, "profiles", "migrate_fast_traffic.txt")
     if os.path.exists(tf):
-        for line in open(tf):
-            if line.startswith("dram_bytes_per_trace_per_column:"):
-                per = float(line.split(":")[1])
-                traffic = per * (npts / nz) * bsz
+        kv = dict(line.split(":", 1) for line in open(tf) if ":" in line and not line.startswith("#"))
+        try:
+            traffic = float(kv["dram_bytes_per_step"]) / float(kv["traces_per_step"]) * bsz
+        except (KeyError, ValueError):
+            traffic = None
 
     if rank == 0:
         per_launch_ms = kernel_ms / a.steps
-        achieved = sfu_rate / 1e12
-        peak = sq.value / 1e12
+        # binding roofline: the special-function unit.  Fixed algorithmic work per
+        # pair: 3 MUFU ops (2 DSR square roots + 1 for the weight sqrt(t)) and 17 FP32
+        # flops, so the pair ceiling is min(MUFU peak / 3, FP32 peak / 17); both
+        # peaks measured now on this GPU (ktmProbePeaks)
+        eval_rate = evaluated / (kernel_ms * 1e-3)
+        # our kernels per step: ktmPrepareTraces (1) + the migration, one launch per
+        # trace block of at most 40 MB of packed samples (ktm_fast.cu)
+        esz = 4 if a.fmt == "f32" else 2
+        blk = max(1024, (40 << 20) // (pitch * esz))
+        nblk = -(-bsz // blk)
+        launches = a.steps * (1 + nblk)
+        pair_peak = min(sq.value / 3.0, 2.0 * fm.value / 17.0)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
@@ -522,19 +549,33 @@ def main():
             "error": {"rel_l2": rel_l2, "max_rel": max_err, "vs": "FP64 device evaluation",
                       "sample": f"{ncols_err} random image columns x {nz} tau, batch 0"},
             "pairs": {"raw_per_step": npts * bsz, "evaluated_fraction": evaluated / max(1, pairs_rank),
-                      "evaluated_rate_gpair_s": evaluated / (kernel_ms * 1e-3) / 1e9},
-            "roofline": {"bound": "sfu", "achieved": achieved, "peak": peak, "unit": "Tsqrt/s",
-                         "frac": achieved / peak,
+                      "evaluated_rate_gpair_s": evaluated / (kernel_ms * 1e-3) / 1e9,
+                      "in_aperture_fraction": in_aperture / max(1, pairs_rank),
+                      "note": "evaluated = in aperture and not past the trace end (kernel "
+                              "counter); in_aperture counted separately in FP64"},
+            "roofline": {"bound": "sfu", "achieved": eval_rate / 1e9, "peak": pair_peak / 1e9,
+                         "unit": "Gpair/s", "frac": eval_rate / pair_peak,
                          "traffic": traffic,
-                         "note": "2 sqrt.approx per evaluated pair over the migrate kernel's "
-                                 "event time; peak = sqrt.approx throughput measured now "
-                                 "(ktmProbePeaks)",
-                         "kernel_ms_per_launch": per_launch_ms},
+                         "algorithmic_bytes": bsz * pitch * (4 if a.fmt == "f32" else 2) + npts * 4,
+                         "definition": "evaluated pairs/s over the migrate kernel's event time; "
+                                       "peak = min(MUFU/3, FP32 flops/17) pairs/s with the "
+                                       "MUFU (sqrt.approx) and FFMA throughputs measured now",
+                         "sfu_issued": {"achieved_tsqrt_s": sfu_rate / 1e12,
+                                        "peak_tsqrt_s": sq.value / 1e12,
+                                        "frac": sfu_rate / sq.value,
+                                        "note": ("2 sqrt.approx per pair, sqrt(t) prefolded into "
+                                                 "the samples" if a.weight == "prefold" else
+                                                 "2 sqrt.approx per pair, plus the weight's "
+                                                 "table lookup or third sqrt.approx")},
+                         "traffic_note": "DRAM read+write of one step (5 launches of the "
+                                         "kernel, one per 40 MB trace block) from one ncu "
+                                         "capture, scaled by traces",
+                         "kernel_ms_per_step": per_launch_ms},
             "peaks_measured": {"sqrt_t_s": sq.value / 1e12, "rsqrt_t_s": rs.value / 1e12,
                                "ffma_t_s": fm.value / 1e12},
             "clocks": clk,
             "e2e": e2e,
-            "gpu_launches": 2 * a.steps,
+            "gpu_launches": launches,
             "cpu_baseline": cpu,
             "setup_s": setup_s,
         }
