@@ -352,6 +352,10 @@ typedef struct ktm_survey {
 } ktm_survey;
 int ktmLoadSurvey(const char* dir, int dataIsIBM, int rebase, ktm_survey* out);
 void ktmFreeSurvey(ktm_survey* s);
+/* velModel.bin (ktmWriteVelModel.m:22-23) for the grid of `inp`: the Nx*Ny*Nz cube
+ * when the file holds exactly that many values, else its first Nz values (the
+ * writer may have appended models).  *velocity is malloc'd (release with free). */
+int ktmReadVelModel(const char* path, const ktm_inp* inp, float** velocity, int* velocityCube);
 /* outputData.bin: float32 [Nx][Ny][Nz], tau fastest (ktmVisualizeOutputFile.m:16-28). */
 int ktmWriteImage(const char* path, const float* image, size_t count);
 
@@ -361,6 +365,76 @@ int ktmWriteImage(const char* path, const float* image, size_t count);
 void ktmIBM32toIEEE(unsigned int* input, float* output, int n);
 /* The same conversion on device buffers, asynchronous on `stream`. */
 int ktmIBM32toIEEEDevice(const unsigned int* input, float* output, size_t n, void* stream);
+
+/* SEG-Y files (rev 0 layout), the C replacement of ktmGetInputMeta.m:21-150 and
+ * ktmGetInputTrace.m:29-75.  Big-endian fields (the standard) unless bigEndian = 0.
+ * Trace-header fields are decoded as signed two's-complement numbers (the scripts'
+ * int32()/int16() casts saturate negative values instead). */
+typedef struct ktm_segy_info {
+    char text[3240];                /* the EBCDIC reel header as ASCII, 40 lines of 80
+                                       characters, '\n'-separated; the characters the
+                                       script's table maps (ktmGetInputMeta.m:30-45),
+                                       '?' for the rest */
+    unsigned int reel32[3];         /* job, line, reel numbers (bytes 3201-3212) */
+    unsigned int reel16[24];        /* the 16-bit binary reel header fields (3213-3260),
+                                       in the order ktmListInputMeta.m names them */
+    int   sampleInterval;           /* us (reel16[2]) */
+    int   samplesPerTrace;          /* reel16[4] */
+    int   format;                   /* reel16[6]: 1 IBM, 2 int32, 3 int16, 5 IEEE, 8 int8 */
+    int   bigEndian;
+    long long traceBytes;           /* 240 + samples * bytes per sample */
+    long long traceCount;           /* whole traces in the file */
+} ktm_segy_info;
+
+typedef struct ktm_segy_trace {
+    int    values[101];             /* the 240-byte header as ktmGetInputMeta.m:132 groups
+                                       it: 7 int32 (bytes 1-28), 4 int16 (29-36), 8 int32
+                                       (37-68), 2 int16 (69-72, [20] = coordinate scalar),
+                                       4 int32 (73-88: [21..24] source x, y, receiver x, y),
+                                       76 int16 (89-240) */
+    double srcX, srcY, recX, recY;  /* coordinates with the scalar applied
+                                       (> 0 multiplier, < 0 divisor, 0 = 1) */
+} ktm_segy_trace;
+
+/* Read the reel headers; the trace count follows from the file size. */
+int ktmSegyOpen(const char* path, int bigEndian, ktm_segy_info* info);
+/* Traces [first, first + count): samples into `samples` ([count][samplesPerTrace]
+ * 4-byte words: IBM words as stored for format 1 -- KTM_FMT_IBM32, decoded on the
+ * GPU -- and float for the other formats) and/or headers (either may be NULL). */
+int ktmSegyReadTraces(const char* path, const ktm_segy_info* info, long long first,
+                      long long count, void* samples, ktm_segy_trace* headers);
+/* KTM_FMT_IBM32 for format 1, KTM_FMT_F32 otherwise (the words ktmSegyReadTraces writes). */
+int ktmSegyTraceFormat(const ktm_segy_info* info);
+/* A survey from traces [first, first + count) of a SEG-Y file (count < 0: to the end):
+ * samples as ktmSegyReadTraces writes them, midpoints / half offsets from the scaled
+ * source and receiver coordinates in FP64 (ktmConvertXYtoOffMid.m:12; rebase = 1
+ * subtracts the survey origin first), tracePts and sampleRate from the reel header.
+ * SEG-Y carries no image grid or velocity: inp.x/y/z and velocity are left zero for
+ * the caller (subtract originX / originY from the x / y starts when rebased).
+ * Release with ktmFreeSurvey. */
+int ktmLoadSegySurvey(const char* path, int bigEndian, long long first, long long count,
+                      int rebase, ktm_survey* out);
+
+/* ------------------------------------------------------------------------ */
+/* Time-axis interpolation (ktmInterpTraceBlock.m:134-154, opt 2)           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct ktm_interp {
+    int   traceNo, tracePts;
+    int   levels;                   /* N: 2^N output samples per input interval (0..10) */
+    const float* in;                /* [traceNo][inStride], device memory */
+    int   inStride;                 /* 0: tracePts */
+    float* out;                     /* [traceNo][outStride], device memory */
+    long long outStride;            /* 0: ktmInterpLength(tracePts, levels) */
+    void* stream;                   /* cudaStream_t */
+} ktm_interp;
+
+/* Samples after interpolation: (tracePts - 1) * 2^levels + 1 (0 for no samples). */
+long long ktmInterpLength(int tracePts, int levels);
+/* Linear interpolation of every trace onto t = j / 2^levels (the new sample
+ * interval is dt / 2^levels), evaluated in FP64 as Octave's interp1 does and
+ * rounded to float: bit-identical to the script on float input.  Asynchronous. */
+int ktmInterpTraces(const ktm_interp* interp);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic data and measurement                                           */

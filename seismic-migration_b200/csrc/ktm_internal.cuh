@@ -88,6 +88,9 @@ int prepare_traces(const ktm_prep* p);
 int widen_traces(const void* in, int fmt, const float* scale, int ntr, int nt, int stride,
                  void** out, cudaStream_t s);
 
+// ktm_interp.cu: time-axis interpolation by 2^levels (ktmInterpTraces).
+int interp_traces(const ktm_interp* p);
+
 // ktm_ibm.cu: IBM-32 words -> IEEE float, bit-identical to ktmIBM32toIEEE.
 int ibm_to_ieee(const uint32_t* in, float* out, size_t n, cudaStream_t s);
 

@@ -117,6 +117,42 @@ int ktmWriteInp(const char* path, const ktm_inp* inp)
     return ktm_io_ok();
 }
 
+int ktmReadVelModel(const char* path, const ktm_inp* inp, float** velocity, int* velocityCube)
+{
+    if (!path || !inp || !velocity || !velocityCube) return io_fail(KTM_ERR_ARG, "NULL argument");
+    *velocity = NULL;
+    *velocityCube = 0;
+    FILE* f = fopen(path, "rb");
+    if (!f) return io_fail(KTM_ERR_IO, "cannot open %s", path);
+    long bytes = file_size(f);
+    fclose(f);
+    if (bytes < 0) return io_fail(KTM_ERR_IO, "cannot size %s", path);
+    const size_t nvel = (size_t)bytes / 4;
+    const size_t nz = (size_t)inp->z.imagePnts;
+    const size_t ncube = (size_t)inp->x.imagePnts * inp->y.imagePnts * nz;
+    /* the cube when the file holds exactly Nx*Ny*Nz values (and that differs from Nz),
+       else the first Nz values (ktmWriteVelModel.m may have appended models) */
+    const int cube = nvel == ncube && ncube != nz;
+    if (!cube && nvel < nz)
+        return io_fail(KTM_ERR_IO, "%s holds %zu values; %zu (1-D) or %zu (cube) expected", path,
+                       nvel, nz, ncube);
+    const char* slash = strrchr(path, '/');
+    char dir[4096];
+    const char* name = path;
+    if (slash) {
+        snprintf(dir, sizeof(dir), "%.*s", (int)(slash - path), path);
+        name = slash + 1;
+    } else {
+        snprintf(dir, sizeof(dir), ".");
+    }
+    void* v = NULL;
+    const int rc = read_words(dir, name, cube ? ncube : nz, &v, NULL);
+    if (rc) return rc;
+    *velocity = (float*)v;
+    *velocityCube = cube;
+    return ktm_io_ok();
+}
+
 void ktmFreeSurvey(ktm_survey* s)
 {
     if (!s) return;
@@ -133,29 +169,21 @@ int ktmLoadSurvey(const char* dir, int dataIsIBM, int rebase, ktm_survey* out)
     int rc = ktmReadInp(path, &out->inp);
     if (rc) return rc;
     const size_t ntr = (size_t)out->inp.traceNo, nt = (size_t)out->inp.tracePts;
-    void *data = NULL, *sx = NULL, *sy = NULL, *rx = NULL, *ry = NULL, *vel = NULL;
-    size_t nvel = 0;
+    void *data = NULL, *sx = NULL, *sy = NULL, *rx = NULL, *ry = NULL;
+    float* vel = NULL;
+    int cube = 0;
+    snprintf(path, sizeof(path), "%s/velModel.bin", dir);
     if ((rc = read_words(dir, "inputData.bin", ntr * nt, &data, NULL)) ||
         (rc = read_words(dir, "inputSrcX.bin", ntr, &sx, NULL)) ||
         (rc = read_words(dir, "inputSrcY.bin", ntr, &sy, NULL)) ||
         (rc = read_words(dir, "inputRecX.bin", ntr, &rx, NULL)) ||
         (rc = read_words(dir, "inputRecY.bin", ntr, &ry, NULL)) ||
-        (rc = read_words(dir, "velModel.bin", 0, &vel, &nvel))) {
+        (rc = ktmReadVelModel(path, &out->inp, &vel, &cube))) {
         free(data); free(sx); free(sy); free(rx); free(ry); free(vel);
         return rc;
     }
-    const size_t nz = (size_t)out->inp.z.imagePnts;
-    const size_t ncube = (size_t)out->inp.x.imagePnts * out->inp.y.imagePnts * nz;
-    if (nvel == ncube && ncube != nz) {
-        out->velocityCube = 1;
-    } else if (nvel >= nz) {
-        out->velocityCube = 0;
-    } else {
-        free(data); free(sx); free(sy); free(rx); free(ry); free(vel);
-        return io_fail(KTM_ERR_IO, "velModel.bin holds %zu values; %zu (1-D) or %zu (cube) expected",
-                       nvel, nz, ncube);
-    }
-    out->velocity = (float*)vel;
+    out->velocityCube = cube;
+    out->velocity = vel;
     out->traces = data;   /* IBM words stay as read: the device converts them */
     out->traceFormat = dataIsIBM ? KTM_FMT_IBM32 : KTM_FMT_F32;
     const float *Sx = (const float*)sx, *Sy = (const float*)sy, *Rx = (const float*)rx,

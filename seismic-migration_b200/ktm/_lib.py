@@ -105,6 +105,26 @@ class KtmSurvey(C.Structure):
                 ("originX", C.c_double), ("originY", C.c_double)]
 
 
+class KtmSegyInfo(C.Structure):
+    """ktm_segy_info (include/ktm.h)."""
+    _fields_ = [("text", C.c_char * 3240), ("reel32", C.c_uint * 3), ("reel16", C.c_uint * 24),
+                ("sampleInterval", C.c_int), ("samplesPerTrace", C.c_int), ("format", C.c_int),
+                ("bigEndian", C.c_int), ("traceBytes", C.c_longlong), ("traceCount", C.c_longlong)]
+
+
+class KtmSegyTrace(C.Structure):
+    """ktm_segy_trace (include/ktm.h)."""
+    _fields_ = [("values", C.c_int * 101), ("srcX", C.c_double), ("srcY", C.c_double),
+                ("recX", C.c_double), ("recY", C.c_double)]
+
+
+class KtmInterp(C.Structure):
+    """ktm_interp (include/ktm.h)."""
+    _fields_ = [("traceNo", C.c_int), ("tracePts", C.c_int), ("levels", C.c_int),
+                ("in_", P), ("inStride", C.c_int), ("out", P), ("outStride", C.c_longlong),
+                ("stream", P)]
+
+
 _lib = None
 
 
@@ -172,6 +192,20 @@ def lib() -> C.CDLL:
     L.ktmIBM32toIEEE.restype = None
     L.ktmIBM32toIEEEDevice.argtypes = [P, P, C.c_size_t, P]
     L.ktmIBM32toIEEEDevice.restype = C.c_int
+    L.ktmSegyOpen.argtypes = [C.c_char_p, C.c_int, C.POINTER(KtmSegyInfo)]
+    L.ktmSegyOpen.restype = C.c_int
+    L.ktmSegyReadTraces.argtypes = [C.c_char_p, C.POINTER(KtmSegyInfo), C.c_longlong,
+                                    C.c_longlong, P, C.POINTER(KtmSegyTrace)]
+    L.ktmSegyReadTraces.restype = C.c_int
+    L.ktmSegyTraceFormat.argtypes = [C.POINTER(KtmSegyInfo)]
+    L.ktmSegyTraceFormat.restype = C.c_int
+    L.ktmLoadSegySurvey.argtypes = [C.c_char_p, C.c_int, C.c_longlong, C.c_longlong, C.c_int,
+                                    C.POINTER(KtmSurvey)]
+    L.ktmLoadSegySurvey.restype = C.c_int
+    L.ktmInterpLength.argtypes = [C.c_int, C.c_int]
+    L.ktmInterpLength.restype = C.c_longlong
+    L.ktmInterpTraces.argtypes = [C.POINTER(KtmInterp)]
+    L.ktmInterpTraces.restype = C.c_int
     _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "

@@ -295,3 +295,24 @@ def migrate_columns_f64(*, columns=None, ncols=None, **kw):
     out = torch.empty((n, nz), device=kw["midX"].device, dtype=torch.float64)
     check(lib().ktmMigrateColumnsF64(C.byref(job.job), _ptr(cols), int(n), out.data_ptr()))
     return out
+
+
+def interp_time(traces, levels: int, stream=None, out=None):
+    """Time-axis interpolation by 2^levels (ktmInterpTraces, ktmInterpTraceBlock.m
+    opt 2): CUDA float32 [traceNo, tracePts] -> [traceNo, (tracePts-1) 2^levels + 1],
+    the new sample interval dt / 2^levels."""
+    import torch
+    if not (_is_torch(traces) and traces.is_cuda and traces.dtype == torch.float32):
+        raise ValueError("interp_time takes a CUDA float32 tensor [traceNo, tracePts]")
+    traces = traces.contiguous()
+    ntr, nt = traces.shape
+    nout = int(lib().ktmInterpLength(int(nt), int(levels)))
+    if out is None:
+        out = torch.empty((ntr, nout), device=traces.device, dtype=torch.float32)
+    p = _lib.KtmInterp()
+    p.traceNo, p.tracePts, p.levels = int(ntr), int(nt), int(levels)
+    p.in_, p.inStride = traces.data_ptr(), int(nt)
+    p.out, p.outStride = out.data_ptr(), int(out.stride(0))
+    p.stream = _stream_handle(stream)
+    check(lib().ktmInterpTraces(C.byref(p)))
+    return out

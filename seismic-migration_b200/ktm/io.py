@@ -7,6 +7,9 @@
     velModel.bin     float32 [Nz] (ktmWriteVelModel.m:22-23) or [Nx][Ny][Nz]
     outputData.bin   float32 [Nx][Ny][Nz], tau fastest
 
+SEG-Y files (``segy_open``, ``read_segy``, ``load_segy_survey``) replace the
+Octave front end ktmGetInputMeta.m / ktmGetInputTrace.m.
+
 ``write_survey`` plays the part of the Octave writers for tests and examples;
 ``load_survey`` is ktmLoadSurvey (ioFunctions.c:94-153 with the coordinate
 conversion of ktmConvertXYtoOffMid.m:12); ``ibm32_to_ieee`` is ktmIBM32toIEEE
@@ -151,3 +154,47 @@ def ibm32_to_ieee(words, stream=None):
         if code:
             raise _lib.KtmError(code, msg)
     return out
+
+
+# ------------------------------------------------------------------------------ SEG-Y ---
+def segy_open(path: str, big_endian: bool = True) -> _lib.KtmSegyInfo:
+    """Reel headers of a SEG-Y file (ktmSegyOpen)."""
+    info = _lib.KtmSegyInfo()
+    check(lib().ktmSegyOpen(os.fsencode(path), int(bool(big_endian)), C.byref(info)))
+    return info
+
+
+def read_segy(path: str, first: int = 0, count: int | None = None, big_endian: bool = True,
+              headers: bool = True):
+    """Traces [first, first + count) of a SEG-Y file (ktmSegyReadTraces).
+    Returns (info, samples, trace headers): samples uint32 IBM words for format 1
+    (decoded on the GPU by the migration or ``ibm32_to_ieee``), float32 otherwise;
+    headers a list of ``ktm_segy_trace`` (or None)."""
+    info = segy_open(path, big_endian)
+    if count is None:
+        count = int(info.traceCount) - first
+    ns = int(info.samplesPerTrace)
+    ibm = lib().ktmSegyTraceFormat(C.byref(info)) == _lib.KTM_FMT_IBM32
+    samples = np.empty((count, ns), np.uint32 if ibm else np.float32)
+    hdr = (_lib.KtmSegyTrace * max(count, 1))() if headers else None
+    check(lib().ktmSegyReadTraces(os.fsencode(path), C.byref(info), int(first), int(count),
+                                  samples.ctypes.data if count else None, hdr))
+    return info, samples, (list(hdr)[:count] if headers else None)
+
+
+def load_segy_survey(path: str, first: int = 0, count: int = -1, big_endian: bool = True,
+                     rebase: bool = False) -> Survey:
+    """A survey from a SEG-Y file (ktmLoadSegySurvey).  The image grid and the
+    velocity are not in the file: ``inp.x/y/z`` are zero and ``velocity`` is empty."""
+    s = _lib.KtmSurvey()
+    check(lib().ktmLoadSegySurvey(os.fsencode(path), int(bool(big_endian)), int(first), int(count),
+                                  int(bool(rebase)), C.byref(s)))
+    try:
+        inp = Inp._from(s.inp)
+        ntr, nt = inp.traceNo, inp.tracePts
+        dt = np.uint32 if s.traceFormat == _lib.KTM_FMT_IBM32 else np.float32
+        traces = _copy(s.traces, ntr * nt, dt).reshape(ntr, nt)
+        co = [_copy(getattr(s, f), ntr, np.float32) for f in ("midX", "midY", "offX", "offY")]
+        return Survey(inp, traces, *co, np.zeros(0, np.float32), (float(s.originX), float(s.originY)))
+    finally:
+        lib().ktmFreeSurvey(C.byref(s))

@@ -10,6 +10,11 @@
  *   --float              inputData.bin holds float32 (the writers' impulse
  *                        option, ktmWriteTraceBlockConstOffset.m:145); the
  *                        default is IBM-32 words (:142), converted on the GPU
+ *   --segy FILE          traces, coordinates (coordinate scalar applied) and the
+ *                        sample interval from a SEG-Y file instead of
+ *                        inputData.bin / inputSrc* / inputRec*; DATA_DIR still
+ *                        gives the image grid (inp.txt) and velModel.bin
+ *   --le                 the SEG-Y file is little-endian
  *   --mode reference     psktmCPU.c arithmetic, bit-identical (default)
  *   --mode fast          the fast kernel (linear pick, FP16 samples, ...)
  *   --pick linear|truncate        fast mode (default linear)
@@ -36,7 +41,7 @@
 static void usage(const char* argv0)
 {
     fprintf(stderr,
-            "usage: %s [--float] [--mode reference|fast] [--pick linear|truncate]\n"
+            "usage: %s [--float] [--segy FILE [--le]] [--mode reference|fast] [--pick linear|truncate]\n"
             "       [--format f32|f16|bf16] [--rho none|2d|2.5d|3d] [--aperture M]\n"
             "       [--rebase|--no-rebase] [-o FILE] [-q] DATA_DIR\n",
             argv0);
@@ -60,6 +65,8 @@ int main(int argc, char** argv)
 {
     const char* dir = NULL;
     const char* outPath = NULL;
+    const char* segy = NULL;
+    int segyLE = 0;
     int isFloat = 0, mode = KTM_MODE_REFERENCE, pick = KTM_PICK_LINEAR, fmt = KTM_FMT_F16;
     int rho = KTM_RHO_NONE, rebase = -1, quiet = 0;
     float aperture = 0.0f;
@@ -68,6 +75,11 @@ int main(int argc, char** argv)
         const char* v = i + 1 < argc ? argv[i + 1] : NULL;
         if (!strcmp(a, "--float")) {
             isFloat = 1;
+        } else if (!strcmp(a, "--le")) {
+            segyLE = 1;
+        } else if (v && !strcmp(a, "--segy")) {
+            segy = v;
+            i++;
         } else if (!strcmp(a, "--rebase")) {
             rebase = 1;
         } else if (!strcmp(a, "--no-rebase")) {
@@ -126,7 +138,25 @@ int main(int argc, char** argv)
 
     const double t0 = now();
     ktm_survey sv;
-    if (ktmLoadSurvey(dir, !isFloat, rebase, &sv)) return fail("reading the survey");
+    if (!segy) {
+        if (ktmLoadSurvey(dir, !isFloat, rebase, &sv)) return fail("reading the survey");
+    } else {
+        char path[4096];
+        ktm_inp grid;
+        snprintf(path, sizeof(path), "%s/inp.txt", dir);
+        if (ktmReadInp(path, &grid)) return fail("reading inp.txt");
+        if (ktmLoadSegySurvey(segy, !segyLE, 0, -1, rebase, &sv)) return fail("reading the SEG-Y file");
+        sv.inp.x = grid.x;
+        sv.inp.y = grid.y;
+        sv.inp.z = grid.z;
+        sv.inp.x.imageStart = (float)((double)grid.x.imageStart - sv.originX);
+        sv.inp.y.imageStart = (float)((double)grid.y.imageStart - sv.originY);
+        snprintf(path, sizeof(path), "%s/velModel.bin", dir);
+        if (ktmReadVelModel(path, &sv.inp, &sv.velocity, &sv.velocityCube)) {
+            ktmFreeSurvey(&sv);
+            return fail("reading velModel.bin");
+        }
+    }
     const double t1 = now();
 
     const size_t nimg = (size_t)sv.inp.x.imagePnts * sv.inp.y.imagePnts * sv.inp.z.imagePnts;
