@@ -55,12 +55,13 @@ def parse():
     ap.add_argument("--ntr", type=int, default=1_000_000)
     ap.add_argument("--batches", type=int, default=16)
     ap.add_argument("--fmt", default="f16", choices=["f16", "bf16", "f32"])
-    ap.add_argument("--err-cols", type=int, default=48)
+    ap.add_argument("--err-side", type=int, default=64,
+                    help="error check on a seeded random SIDE x SIDE x Nz subgrid (FP64 device)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--skip-error", action="store_true", help="skip the FP64 error check")
-    ap.add_argument("--config", default="3d", choices=["3d", "batch"],
+    ap.add_argument("--config", default="3d", choices=["3d", "batch", "2d", "lsm"],
                     help="3d: the headline workload; batch: 64 target-oriented jobs in one "
                          "persistent launch")
     ap.add_argument("--jobs", type=int, default=64)
@@ -201,7 +202,8 @@ def batch_main(a):
     uniform over the patch grown by the 2 km aperture, offsets <= 3150 m, the
     line survey's Vrms(t0) = 1500 + 0.5 t0[ms], 25 Hz Ricker diffractions from
     20 scatterers plus sigma 0.05 noise, 2.5-D rho filter, BF16 traces with an
-    FP32 scale, FP32 accumulation, tau-run length from ktmAutotune.  Then the
+    FP32 scale and sqrt(j dt) folded in, FP32 accumulation, tau-run length from
+    ktmAutotune.  Then the
     error of sampled jobs against the FP64 device evaluation, and 10-iteration
     CGLS (one iteration captured in a CUDA graph) on the smallest jobs."""
     import torch
@@ -227,7 +229,7 @@ def batch_main(a):
         sv.imageX.imageStart = sv.imageY.imageStart = 2000.0 + 6.25
         coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
         raw = synth.synthesize_device(sv, device=dev, coords=coords)
-        packed = ktm.prepare(raw, sv.dt, fmt="bf16", rho=sv.rho_opt, prefold=False)
+        packed = ktm.prepare(raw, sv.dt, fmt="bf16", rho=sv.rho_opt, prefold=True)
         del raw
         jobs.append(dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
                          midX=coords[0], midY=coords[1], offX=coords[2], offY=coords[3],
@@ -282,11 +284,176 @@ def batch_main(a):
         "metric": METRIC, "config": {"workload": f"batched: {len(jobs)} jobs in one persistent launch",
                                      "patch_sides": [s.shape[0] for s in surveys],
                                      "traces": [s.ntr for s in surveys], "nz": 751,
-                                     "trace_format": "bf16", "tile_run": run},
+                                     "trace_format": "bf16", "tile_run": run,
+                                     "weight": "sqrt(j dt) folded into the packed samples"},
         "value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_launch": ms, "pairs": pairs,
         "steps": len(times), "error_rel_l2": {"max": max(errs), "median": float(np.median(errs)),
                                                "jobs": len(errs), "vs": "FP64 device, 32 columns per job"},
         "lsm_10_iterations": lsm, "setup_s": setup_s,
+    }), flush=True)
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def line_main(a):
+    """The 2-D line (256 CMPs x 64 offsets, 16,384 traces of 1001 samples at 4 ms,
+    256 x 1001 image, aperture 2 km, 2.5-D rho filter) in FP32, FP16 and BF16 with a
+    per-trace FP32 scale (prefolded weight): throughput of each, its relative L2 and
+    max error against the FP64 device evaluation of the WHOLE image, the plain FP32
+    (bit-exact psktmCPU.c arithmetic) kernel on the same traces, and the reference's
+    own psktmCPU.c on all host threads over the whole job."""
+    import torch
+
+    import ktm
+    from ktm import synth
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sv = synth.config1()
+    T = lambda x: torch.as_tensor(np.ascontiguousarray(x, dtype=np.float32)).to(dev)  # noqa: E731
+    coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    raw = synth.synthesize_device(sv, device=dev, coords=coords)
+    vel = T(sv.velocity1d)
+    nx, ny, nz = sv.shape
+    npts = nx * ny * nz
+    geo = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt, midX=coords[0],
+               midY=coords[1], offX=coords[2], offY=coords[3], velocity=vel,
+               aperture=sv.aperture)
+    p32 = ktm.prepare(raw, sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
+    ref = ktm.migrate_columns_f64(ncols=nx * ny, traces=p32, pick="linear", **geo).double()
+    out = {}
+    for fmt in ("f32", "f16", "bf16"):
+        p = ktm.prepare(raw, sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
+        img = torch.empty(sv.shape, device=dev, dtype=torch.float32)
+        for _ in range(max(3, a.warmup)):
+            ktm.migrate(traces=p, image=img, pick="linear", **geo)
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(a.steps):
+            ktm.migrate(traces=p, image=img, pick="linear", **geo)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        got = img.reshape(nx * ny, nz).double()
+        out[fmt] = {"gpair_s": npts * sv.ntr / (ms * 1e-3) / 1e9, "ms": ms,
+                    "rel_l2": float((got - ref).norm() / ref.norm()),
+                    "max_rel": float((got - ref).abs().max() / ref.abs().max())}
+    # the mixed kernel on the same work as the plain one (no aperture: every pair)
+    p16 = ktm.prepare(raw, sv.dt, fmt="f16", rho=sv.rho_opt, prefold=True)
+    img = torch.empty(sv.shape, device=dev, dtype=torch.float32)
+    nokw = dict(geo, aperture=0.0)
+    for _ in range(3):
+        ktm.migrate(traces=p16, image=img, pick="linear", **nokw)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(a.steps):
+        ktm.migrate(traces=p16, image=img, pick="linear", **nokw)
+    e1.record()
+    torch.cuda.synchronize()
+    f16_all = npts * sv.ntr / (e0.elapsed_time(e1) / a.steps * 1e-3) / 1e9
+    # plain FP32: the reference-mode kernel (truncating pick, rho-free traces as psktmCPU.c takes them)
+    pimg = torch.empty(sv.shape, device=dev, dtype=torch.float32)
+    plain_kw = dict(geo, traces=raw, mode="reference", pick="truncate", aperture=0.0, image=pimg)
+    for _ in range(3):
+        ktm.migrate(**plain_kw)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(a.steps):
+        ktm.migrate(**plain_kw)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / a.steps
+    plain = npts * sv.ntr / (plain_ms * 1e-3) / 1e9
+    cpu = None
+    if not a.no_cpu_baseline:
+        r, cores, kind, sample = cpu_reference_rate(sv, a.cpu_seconds, os.cpu_count() or 1)
+        cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    print(json.dumps({
+        "metric": METRIC, "value": out["f16"]["gpair_s"], "unit": UNIT, "n_gpus": 1,
+        "steps": a.steps, "higher_is_better": True, "dtype": "f16 traces, f32 accumulate",
+        "data": "synthetic (seeded, device-generated)",
+        "config": {"workload": "2-D line: 256 CMPs x 64 offsets (16,384 traces x 1001 samples "
+                               "at 4 ms), 256 x 1001 image, aperture 2 km, 2.5-D rho",
+                   "weight": "sqrt(j dt) folded into the packed samples"},
+        "formats": out, "error_vs": "FP64 device evaluation of the whole image",
+        "plain_fp32": {"value": plain, "unit": UNIT, "ms": plain_ms,
+                       "mixed_over_plain": {f: out[f]["gpair_s"] / plain for f in out},
+                       "f16_no_aperture_gpair_s": f16_all,
+                       "mixed_over_plain_same_work": f16_all / plain},
+        "cpu_baseline": cpu,
+    }), flush=True)
+
+
+def lsm_main(a):
+    """Adjoint and least squares on the 2-D line of 512 CMPs x 64 offsets x 1001
+    samples at 4 ms (FP32): the dot-product test <L m, d> = <m, L^T d> with seeded
+    Gaussian m and d, 20 CGLS iterations (graph-captured) on data demigrated from a
+    seeded sparse reflectivity (5 % non-zeros, N(0,1)), and the Vrms gradient
+    against central finite differences of the device image (eps = 1e-3 v)."""
+    import torch
+
+    from ktm import synth
+    from ktm.inverse import MigrationOperator
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    sv = synth.config4()
+    T = lambda x: torch.as_tensor(np.ascontiguousarray(x, dtype=np.float32)).to(dev)  # noqa: E731
+    coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    kw = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt, nt=sv.nt,
+              midX=coords[0], midY=coords[1], offX=coords[2], offY=coords[3],
+              aperture=sv.aperture)
+    op = MigrationOperator(velocity=T(sv.velocity1d), **kw)
+    rng = np.random.default_rng(4)
+    m = T(rng.standard_normal(op.shape))
+    d = op.pack(T(rng.standard_normal((sv.ntr, sv.nt))))
+    Lm = op.demigrate(m)
+    LTd = op.migrate(d)
+    lhs = float((Lm.double() * d.double()).sum())
+    rhs = float((m.double() * LTd.double()).sum())
+    # operator timings
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+    demig_ms = timed(lambda: op.demigrate(m, data=Lm))
+    mig_ms = timed(lambda: op.migrate(d, image=LTd))
+    m_true = T(np.where(rng.uniform(size=op.shape) < 0.05, rng.standard_normal(op.shape), 0.0))
+    dobs = op.demigrate(m_true)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model, rn, gn = op.least_squares(dobs, 20, use_graph=True)
+    torch.cuda.synchronize()
+    lsm_s = time.perf_counter() - t0
+    # gradient vs central differences on a band-limited data set
+    tr = synth.synthesize_device(sv, device=dev, coords=coords)
+    cube = T(np.broadcast_to(sv.velocity1d, op.shape))
+    gop = MigrationOperator(velocity=cube, **kw)
+    packed = gop.pack(tr)
+    eps = 1e-3
+    opp = MigrationOperator(velocity=cube * (1 + eps), **kw)
+    opm = MigrationOperator(velocity=cube * (1 - eps), **kw)
+    fd = (opp.migrate(packed) - opm.migrate(packed)).double() / (2 * eps * cube.double())
+    g = gop.vrms_gradient(gop.packed(packed)).double()
+    npairs = op.shape[0] * op.shape[1] * op.shape[2] * sv.ntr
+    print(json.dumps({
+        "metric": "adjoint / LSM, 2-D line 512 CMPs x 64 offsets x 1001 samples",
+        "config": {"workload": "2-D line: 32,768 traces x 1001 samples at 4 ms, 512 x 1001 image, "
+                               "aperture 2 km, FP32, linear pick, table weight"},
+        "dot_test": {"lhs": lhs, "rhs": rhs, "rel_diff": abs(lhs - rhs) / abs(lhs)},
+        "demigrate_ms": demig_ms, "migrate_ms": mig_ms,
+        "demigrate_gpair_s": npairs / (demig_ms * 1e-3) / 1e9,
+        "migrate_gpair_s": npairs / (mig_ms * 1e-3) / 1e9,
+        "lsm_20": {"seconds": lsm_s, "residual_ratio": float(rn[-1] / rn[0]),
+                   "gradient_ratio": float(gn[-1] / gn[0]), "graph": True},
+        "vrms_gradient_vs_fd": {"rel_l2": float((g - fd).norm() / fd.norm()), "eps": eps},
     }), flush=True)
 
 
@@ -297,6 +464,12 @@ def main():
         return
     if a.config == "batch":
         batch_main(a)
+        return
+    if a.config == "2d":
+        line_main(a)
+        return
+    if a.config == "lsm":
+        lsm_main(a)
         return
     import torch
 
@@ -422,7 +595,7 @@ def main():
     # ---- accuracy: one batch, fresh image, vs FP64 device evaluation (rho-filtered
     # FP32 input, weight |tau| sqrt(t) per pair) on sampled columns
     rel_l2 = max_err = None
-    ncols_err = 0
+    ncols_err = (0, 0)
     if not a.skip_error:
         k0, k1 = bounds[0]
         image_keep = image.clone()
@@ -431,9 +604,10 @@ def main():
         stream.synchronize()
         p32 = ktm.prepare(raw[k0:k1], sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
         rng = np.random.default_rng(17)
-        cols = torch.as_tensor(rng.choice(nx * ny, size=min(a.err_cols, nx * ny), replace=False)
-                               .astype(np.int32))
-        ncols_err = len(cols)
+        xs = np.sort(rng.choice(nx, size=min(a.err_side, nx), replace=False))
+        ys = np.sort(rng.choice(ny, size=min(a.err_side, ny), replace=False))
+        cols = torch.as_tensor((xs[:, None] * ny + ys[None, :]).ravel().astype(np.int32))
+        ncols_err = (len(xs), len(ys))
         ref = ktm.migrate_columns_f64(
             columns=cols, imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
             midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
@@ -543,11 +717,16 @@ def main():
                        "l2": "each step reads a new 375 MB batch (> 126 MB L2)",
                        "parallelism": f"{world} GPU(s), one image tile per GPU, no collective"},
             "plain_fp32": {"value": plain_rate, "unit": UNIT,
-                           "kernel": "bit-exact psktmCPU.c arithmetic",
+                           "kernel": "bit-exact psktmCPU.c arithmetic (no aperture: every pair)",
                            "sample": f"{kp} traces x full image, 1-D velocity",
-                           "mixed_over_plain": value / world / plain_rate},
+                           "mixed_over_plain": value / world / plain_rate,
+                           "mixed_over_plain_same_work": (evaluated / (kernel_ms * 1e-3) / 1e9)
+                                                         / plain_rate,
+                           "same_work_note": "evaluated (in-aperture) pairs/s of the mixed "
+                                             "kernel over the plain kernel's pairs/s"},
             "error": {"rel_l2": rel_l2, "max_rel": max_err, "vs": "FP64 device evaluation",
-                      "sample": f"{ncols_err} random image columns x {nz} tau, batch 0"},
+                      "sample": f"seeded random {ncols_err[0]}x{ncols_err[1]}x{nz} subgrid, "
+                                f"batch 0 ({bsz} traces)"},
             "pairs": {"raw_per_step": npts * bsz, "evaluated_fraction": evaluated / max(1, pairs_rank),
                       "evaluated_rate_gpair_s": evaluated / (kernel_ms * 1e-3) / 1e9,
                       "in_aperture_fraction": in_aperture / max(1, pairs_rank),
