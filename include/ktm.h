@@ -149,7 +149,8 @@ typedef struct ktm_job {
                                                   0: host memory, copied in and out */
     void* stream;                              /* cudaStream_t (NULL: legacy default) */
     int   tileRun;                             /* tau samples per thread (0: tuned) */
-    int   tileCols;                            /* image columns per CTA (0: tuned) */
+    int   tileCols;                            /* not read: a fast-kernel CTA always covers
+                                                  8 image columns (one per warp); keep 0 */
     unsigned long long* pairsEvaluated;        /* optional device counter: pairs the
                                                   kernel evaluated (after culling) */
     /* FAST mode with raw (not packed) traces: the library prepares them first */

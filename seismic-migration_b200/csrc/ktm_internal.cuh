@@ -49,8 +49,9 @@ struct FastArgs {
     const float* midX; const float* midY; const float* offX; const float* offY;
     const void* traces; const float* scale; int fmt;
     int pitch;              // elements between traces
-    // FP64 reference only: 0 weight |tau| sqrt(t) per pair; 1 sqrt(j*dt) applied
-    // to each sample; 2 samples already carry sqrt(j*dt)
+    // 0: the kernel evaluates |tau| sqrt(t) per pair (weightMethod says how);
+    // 1: sqrt(j*dt) applied to each sample (FP64 device reference only);
+    // 2: the packed samples already carry sqrt(j*dt)
     int weightMode;
     int weightMethod;       // KTM_WEIGHT_* when the samples do not carry sqrt(j*dt)
     const float* vel; int velCube;
