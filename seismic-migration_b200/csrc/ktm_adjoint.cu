@@ -13,9 +13,11 @@
 // in shared memory (red.shared.add) while its warps sweep the image columns of
 // its column block, and writes the chunk out once (plain stores when one block
 // covers all columns, red.global.add otherwise).  A warp covers one column x a
-// run of 32*R tau samples at a time, as in the migration; the model samples,
-// the tau tables and the velocity of the run stay in registers for all the
-// chunk's traces.
+// run of 32*R tau samples at a time; the model samples, the tau tables and the
+// velocity of the run stay in registers for all the chunk's traces.  FP32
+// shared atomics run at ~7 per clock per SM on distinct addresses and serialise
+// on equal ones, so each lane merges its own contributions before issuing them
+// (demigrate_merge_kernel).
 #include "ktm_pair.cuh"
 
 #include <algorithm>
@@ -51,34 +53,18 @@ __device__ __forceinline__ void red_shared(unsigned addr, float v)
     asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(addr), "f"(v));
 }
 
-// Scatter-add from the 32 lanes of a warp.  FP32 shared-memory atomics run at
-// ~7 per clock per SM on distinct addresses but serialise on equal ones (0.3
-// per clock at 32 lanes per address, measured on B200) -- and the lanes of a
-// warp hold consecutive tau samples of one trace, so where t(tau) is flat
-// (shallow, far offsets) runs of lanes hit the same sample.  When a warp has
-// such a run, the run is summed into its first lane by a segmented suffix sum
-// (five shuffles) and only that lane issues the atomic.
-__device__ __forceinline__ void scatter_add(unsigned addr, float v, int lane)
-{
-    const unsigned prev = __shfl_up_sync(0xffffffffu, addr, 1);
-    const bool dup = lane > 0 && prev == addr;
-    if (!__any_sync(0xffffffffu, dup)) {
-        red_shared(addr, v);
-        return;
-    }
-    const unsigned heads = __ballot_sync(0xffffffffu, !dup);
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float t = __shfl_down_sync(0xffffffffu, v, o);
-        // lane + o belongs to this lane's run iff no run starts in (lane, lane + o]
-        if (lane + o < 32 && ((heads >> (lane + 1)) & ((1u << o) - 1u)) == 0u) v += t;
-    }
-    if (!dup) red_shared(addr, v);
-}
-
+// Lane-private merge of the scatter: lane L owns the 16 CONSECUTIVE tau samples run0 + 16 L + i of a run, so for one trace
+// the target sample floor(u) advances monotonically (mostly by 0 or 1) along
+// the lane's samples.  The lane walks them keeping a running (sample, value,
+// value of the next sample) and issues an atomic only when it leaves a sample:
+// one red.shared per pair where u advances by a sample, fewer where it stalls
+// (shallow, far offsets), two only where it jumps.  Lane L visits its samples
+// starting at i = L mod 16 (slot s holds sample (s + L) mod 16), so at each step
+// the 32 lanes sit 17 samples apart and hit distinct banks; the one wrap per lane
+// is an ordinary jump.
 template <int PICK, int WT>
 __global__ void __launch_bounds__(kAdjThreads)
-demigrate_kernel(AdjArgs a)
+demigrate_merge_kernel(AdjArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Geometry& g = a.g;
@@ -119,7 +105,7 @@ demigrate_kernel(AdjArgs a)
         const int ci = col / g.ny, cj = col % g.ny;
         const float cx = g.x0 + (float)ci * g.dx, cy = g.y0 + (float)cj * g.dy;
         for (int run = 0; run < nruns; run++) {
-            const int run0 = run * 32 * kAdjR;
+            const int base = run * 32 * kAdjR + kAdjR * lane;      // the lane's first sample
             f2 T2[kAdjR / 2], S2[kAdjR / 2], MT[kAdjR / 2];
             float t2min = 3.0e38f, smin = 3.0e38f;
             bool any = false;
@@ -128,7 +114,7 @@ demigrate_kernel(AdjArgs a)
                 float tv[2], sv[2], mv[2];
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
-                    const int l = run0 + lane + 32 * (2 * h + e);
+                    const int l = base + ((2 * h + e + lane) & (kAdjR - 1));
                     const bool ok = l < g.nz;
                     const int lc = ok ? l : g.nz - 1;
                     const float tau = g.z0 + (float)lc * g.dz;
@@ -137,7 +123,6 @@ demigrate_kernel(AdjArgs a)
                     const float vd = v * g.dt;
                     tv[e] = tq * tq;
                     sv[e] = 1.0f / (vd * vd);
-                    // |tau| m[p]: the per-image-sample factor of the weight
                     mv[e] = ok ? fabsf(tau) * a.image[(size_t)col * g.nz + l] : 0.0f;
                     if (ok) { t2min = fminf(t2min, tv[e]); smin = fminf(smin, sv[e]); }
                     any |= (mv[e] != 0.0f);
@@ -159,15 +144,12 @@ demigrate_kernel(AdjArgs a)
                 if (ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2) continue;
                 const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
                 const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
-                // conservative bound (approximate square roots; the margin covers them)
                 const float ulb = sqrt_approx(fmaf(ds, smin, t2min)) + sqrt_approx(fmaf(dr, smin, t2min));
                 if (!(ulb < umax * 1.0001f + 1.0f)) continue;   // past the trace end (warp-uniform)
                 const unsigned rowS = accS + (unsigned)(c * a.pitch) * 4u;
                 const f2 DS = pk(ds, ds), DR = pk(dr, dr);
-                // phase 1: kinematics, weights and contributions of all the lane's pairs
-                // (the table loads pipeline back to back); phase 2: the scatter
-                unsigned adr[kAdjR];
-                float ca[kAdjR], cb[kAdjR];
+                unsigned qc = 0u;
+                float va = 0.0f, vb = 0.0f;
 #pragma unroll
                 for (int h = 0; h < kAdjR / 2; h++) {
                     const PairKin kk = pair_kin(DS, DR, S2[h], T2[h], umax, M2);
@@ -180,28 +162,40 @@ demigrate_kernel(AdjArgs a)
                                  pk(sqrtf(g.dt), sqrtf(g.dt)));
                     }
                     const f2 VAL = mul2(W, MT[h]);
-                    adr[2 * h] = rowS + kk.q0 * 4u;
-                    adr[2 * h + 1] = rowS + kk.q1 * 4u;
+                    float ca[2], cb[2];
                     if (PICK == KTM_PICK_LINEAR) {
-                        const f2 B = mul2(VAL, kk.F);          // f * val
-                        const f2 A = sub2(VAL, B);             // (1 - f) * val
-                        upk(A, ca[2 * h], ca[2 * h + 1]);
-                        upk(B, cb[2 * h], cb[2 * h + 1]);
+                        const f2 B = mul2(VAL, kk.F);          // f * val       -> sample i0 + 1
+                        const f2 A = sub2(VAL, B);             // (1 - f) * val -> sample i0
+                        upk(A, ca[0], ca[1]);
+                        upk(B, cb[0], cb[1]);
                     } else {
-                        upk(VAL, ca[2 * h], ca[2 * h + 1]);
+                        upk(VAL, ca[0], ca[1]);
+                        cb[0] = cb[1] = 0.0f;
+                    }
+                    const unsigned qs[2] = {rowS + kk.q0 * 4u, rowS + kk.q1 * 4u};
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        const unsigned q = qs[e];
+                        if (h == 0 && e == 0) {
+                            qc = q; va = ca[0]; vb = cb[0];
+                            continue;
+                        }
+                        const bool same = q == qc;
+                        const bool next = q == qc + 4u;
+                        if (!same) red_shared(qc, va);
+                        if (PICK == KTM_PICK_LINEAR && !same && !next) red_shared(qc + 4u, vb);
+                        va = same ? va + ca[e] : (next ? vb + ca[e] : ca[e]);
+                        vb = same ? vb + cb[e] : cb[e];
+                        qc = q;
                     }
                 }
-#pragma unroll
-                for (int r = 0; r < kAdjR; r++) {
-                    scatter_add(adr[r], ca[r], lane);
-                    if (PICK == KTM_PICK_LINEAR) scatter_add(adr[r] + 4u, cb[r], lane);
-                }
+                red_shared(qc, va);
+                if (PICK == KTM_PICK_LINEAR) red_shared(qc + 4u, vb);
             }
         }
     }
     asm volatile("" ::: "memory");     // the scatter wrote acc: no load below reuses older values
     __syncthreads();
-    // out: samples 0 < j < nt; the guards absorbed the pairs that read zero guards
     for (int i = threadIdx.x; i < n * a.pitch; i += kAdjThreads) {
         const int c = i / a.pitch, j = i % a.pitch;
         const float v = (j > 0 && j < g.nt) ? acc[i] : 0.0f;
@@ -256,9 +250,9 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
     dim3 grid((unsigned)chunks, (unsigned)blocks);
 #define KTM_ADJ_LAUNCH(P, W)                                                                    \
     do {                                                                                        \
-        KTM_CUDA_TRY(cudaFuncSetAttribute(demigrate_kernel<P, W>,                              \
+        KTM_CUDA_TRY(cudaFuncSetAttribute(demigrate_merge_kernel<P, W>,                        \
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        demigrate_kernel<P, W><<<grid, kAdjThreads, smem, s>>>(a);                             \
+        demigrate_merge_kernel<P, W><<<grid, kAdjThreads, smem, s>>>(a);                       \
     } while (0)
     const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : 0;
     if (pick == KTM_PICK_LINEAR) {
