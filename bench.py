@@ -666,6 +666,10 @@ def main():
         stream.synchronize()
         wall = time.perf_counter() - t0
         e_ms = max(he0.elapsed_time(he1), wall * 1e3) / a.e2e_steps
+        if dist:                                   # the slowest rank's time, as for value
+            t = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
         h2d = n * sv.nt * 4 + 4 * n * 4 + vel.numel() * 4
         e2e = {"value": npts * n / (e_ms * 1e-3) / 1e9 * world, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 4),
