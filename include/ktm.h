@@ -437,6 +437,14 @@ long long ktmInterpLength(int tracePts, int levels);
  * rounded to float: bit-identical to the script on float input.  Asynchronous. */
 int ktmInterpTraces(const ktm_interp* interp);
 
+/* The library keeps its temporary device memory (the device copies of host-memory
+ * jobs, packing buffers, trace-slice partial images, the least-squares workspace)
+ * in a memory pool of its own per device that holds on to freed memory, so
+ * repeated calls do not map memory again.  This returns that memory to the
+ * device; it synchronises every device the library has used.  No counterpart in
+ * the reference. */
+int ktmReleaseMemory(void);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic data and measurement                                           */
 /* ------------------------------------------------------------------------ */

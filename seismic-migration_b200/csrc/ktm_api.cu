@@ -34,6 +34,42 @@ int set_ok()
 }
 
 namespace {
+constexpr int kPoolDevices = 64;
+std::mutex g_poolMu;
+cudaMemPool_t g_pool[kPoolDevices];
+bool g_poolTried[kPoolDevices];
+}  // namespace
+
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = nullptr;
+    if (dev >= 0 && dev < kPoolDevices) {
+        std::lock_guard<std::mutex> lk(g_poolMu);
+        if (!g_poolTried[dev]) {
+            g_poolTried[dev] = true;
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created = nullptr;
+            if (cudaMemPoolCreate(&created, &props) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep);
+                g_pool[dev] = created;
+            } else {
+                cudaGetLastError();
+            }
+        }
+        pool = g_pool[dev];
+    }
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
+namespace {
 
 bool grid_ok(const imageGrid& g) { return g.imagePnts >= 0; }
 
@@ -74,7 +110,7 @@ struct Staged {
     {
         *p = nullptr;
         if (bytes == 0) return KTM_OK;
-        KTM_CUDA_TRY(cudaMallocAsync(p, bytes, s));
+        KTM_CUDA_TRY(pool_malloc(p, bytes, s));
         ptrs.push_back(*p);
         return KTM_OK;
     }
@@ -109,7 +145,7 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         // IBM words: convert on the device (ioFunctions.c:4-40), then migrate
         const size_t n = (size_t)g.ntr * g.stride;
         void* conv = nullptr;
-        if (n) KTM_CUDA_TRY(cudaMallocAsync(&conv, n * 4, s));
+        if (n) KTM_CUDA_TRY(pool_malloc(&conv, n * 4, s));
         int rc = ibm_to_ieee(static_cast<const uint32_t*>(traces), static_cast<float*>(conv), n, s);
         if (!rc)
             rc = launch_reference(g, midX, midY, offX, offY, static_cast<const float*>(conv), vel,
@@ -162,8 +198,8 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         }
         const int pitch = packed_pitch(g.nt, j->packFormat);
         const size_t esize = j->packFormat == KTM_FMT_F32 ? 4 : 2;
-        cudaError_t e = cudaMallocAsync(&packed, (size_t)g.ntr * pitch * esize, s);
-        if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&pscale), (size_t)g.ntr * 4, s);
+        cudaError_t e = pool_malloc(&packed, (size_t)g.ntr * pitch * esize, s);
+        if (e == cudaSuccess) e = pool_malloc(reinterpret_cast<void**>(&pscale), (size_t)g.ntr * 4, s);
         if (e != cudaSuccess) {
             rc = set_error(KTM_ERR_NOMEM, "fast path: packing buffer: %s", cudaGetErrorString(e));
         } else {
@@ -273,6 +309,25 @@ void dropin(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* 
 }  // namespace ktm
 
 extern "C" {
+
+int ktmReleaseMemory(void)
+{
+    std::lock_guard<std::mutex> lk(ktm::g_poolMu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d = 0; d < ktm::kPoolDevices; d++) {
+        if (!ktm::g_pool[d]) continue;
+        cudaError_t e = cudaSetDevice(d);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemPoolTrimTo(ktm::g_pool[d], 0);
+        if (e != cudaSuccess) {
+            cudaSetDevice(cur);
+            return ktm::set_error(KTM_ERR_CUDA, "ktmReleaseMemory: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaSetDevice(cur);
+    return ktm::set_ok();
+}
 
 // status hooks of the host-side file I/O (ktm_io.c)
 int ktm_io_error(int code, const char* msg) { return ktm::set_error(code, "%s", msg); }

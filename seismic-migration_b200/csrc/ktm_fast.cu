@@ -409,7 +409,7 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
         if (a.scratch && a.scratchBytes >= (size_t)slices * nimg * sizeof(float)) {
             partial = static_cast<float*>(a.scratch);
         } else {
-            KTM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&partial),
+            KTM_CUDA_TRY(pool_malloc(reinterpret_cast<void**>(&partial),
                                          (size_t)slices * nimg * sizeof(float), stream));
         }
     }
@@ -672,7 +672,7 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
     const size_t bTiles = sizeof(BatchTile) * sorted.size();
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
     unsigned char* buf = nullptr;
-    KTM_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&buf), up(bJobs) + up(bChunks) + up(bTiles) + 256, s));
+    KTM_CUDA_TRY(pool_malloc(reinterpret_cast<void**>(&buf), up(bJobs) + up(bChunks) + up(bTiles) + 256, s));
     FastArgs* dJobs = reinterpret_cast<FastArgs*>(buf);
     int* dChunks = reinterpret_cast<int*>(buf + up(bJobs));
     BatchTile* dTiles = reinterpret_cast<BatchTile*>(buf + up(bJobs) + up(bChunks));

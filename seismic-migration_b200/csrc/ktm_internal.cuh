@@ -78,6 +78,12 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
                      float* data, int pitch, int pick, int weightMethod, float aperture,
                      int accumulate, cudaStream_t s);
 
+// ktm_api.cu: stream-ordered temporary allocations from the library's own memory
+// pool on the current device (release threshold unlimited, so repeated calls
+// reuse the memory instead of mapping it again; ktmReleaseMemory trims it).
+// Falls back to the device's default pool if a pool cannot be created.
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s);
+
 // ktm_api.cu: geometry of a job (validates sizes)
 int job_geometry(const ktm_job* j, Geometry* g);
 

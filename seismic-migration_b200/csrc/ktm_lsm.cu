@@ -222,7 +222,7 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
     const size_t bytes = 2 * s.nd * 4 + 2 * s.nm * 4 + (size_t)s.g.ntr * 4 + s.scratchBytes +
                          (kDotBlocks + kNScalars + 2 * (its + 1)) * sizeof(double) + 1024;
     unsigned char* ws = nullptr;
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ws), bytes, s.st);
+    cudaError_t e = pool_malloc(reinterpret_cast<void**>(&ws), bytes, s.st);
     if (e != cudaSuccess) {
         if (ownStream) cudaStreamDestroy(s.st);
         return set_error(KTM_ERR_NOMEM, "ktmLeastSquaresMigrate: workspace of %zu bytes: %s", bytes,

@@ -237,7 +237,7 @@ int widen_traces(const void* in, int fmt, const float* scale, int ntr, int nt, i
     *out = nullptr;
     const size_t n = (size_t)ntr * nt;
     if (n == 0) return KTM_OK;
-    KTM_CUDA_TRY(cudaMallocAsync(out, n * sizeof(float), s));
+    KTM_CUDA_TRY(pool_malloc(out, n * sizeof(float), s));
     const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 65535 * 8);
     widen_kernel<<<blocks, 256, 0, s>>>(in, fmt, scale, ntr, nt, stride, static_cast<float*>(*out));
     KTM_CUDA_TRY(cudaGetLastError());

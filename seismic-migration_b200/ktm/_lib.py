@@ -206,6 +206,8 @@ def lib() -> C.CDLL:
     L.ktmInterpLength.restype = C.c_longlong
     L.ktmInterpTraces.argtypes = [C.POINTER(KtmInterp)]
     L.ktmInterpTraces.restype = C.c_int
+    L.ktmReleaseMemory.argtypes = []
+    L.ktmReleaseMemory.restype = C.c_int
     _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "

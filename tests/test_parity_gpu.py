@@ -387,3 +387,20 @@ def test_fast_trace_blocks_for_large_sets(cuda, ktm_lib):
                               np.ascontiguousarray(q[:, :nt]), vel, pick=1, prefold=2)
     assert rel_l2(img, same) < 2e-5
     assert 0 < int(c.item()) <= ntr * 3 * 2 * 120
+
+
+def test_memory_pool_reuse_and_release(cuda, ktm_lib):
+    """Temporaries come from the library's own pool: repeated host-memory calls give
+    the same image, and ktmReleaseMemory hands the pool back without breaking the
+    next call."""
+    import ktm
+    case = random_case(19, ntr=300, nx=6, ny=4, nz=200, data="ricker")
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    kw = dict(imageX=gx, imageY=gy, imageZ=gz, dt=dt, midX=mx, midY=my, offX=ox, offY=oy,
+              traces=tr, velocity=vel, pick="linear", rho=3, pack_format="f16", weight="prefold")
+    a = ktm.migrate(**kw)
+    b = ktm.migrate(**kw)
+    assert np.array_equal(a, b)
+    assert ktm_lib.ktmReleaseMemory() == 0
+    c = ktm.migrate(**kw)
+    assert np.array_equal(a, c)
