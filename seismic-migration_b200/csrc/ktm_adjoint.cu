@@ -52,6 +52,12 @@ __device__ __forceinline__ void red_shared(unsigned addr, float v)
 {
     asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(addr), "f"(v));
 }
+// The same, issued only where `on` holds: a predicated instruction, no branch.
+__device__ __forceinline__ void red_shared_if(bool on, unsigned addr, float v)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p red.shared.add.f32 [%0], %1;\n\t}"
+                 ::"r"(addr), "f"(v), "r"((unsigned)on));
+}
 
 // Lane-private merge of the scatter: lane L owns the 16 CONSECUTIVE tau samples run0 + 16 L + i of a run, so for one trace
 // the target sample floor(u) advances monotonically (mostly by 0 or 1) along
@@ -182,8 +188,8 @@ demigrate_merge_kernel(AdjArgs a)
                         }
                         const bool same = q == qc;
                         const bool next = q == qc + 4u;
-                        if (!same) red_shared(qc, va);
-                        if (PICK == KTM_PICK_LINEAR && !same && !next) red_shared(qc + 4u, vb);
+                        red_shared_if(!same, qc, va);
+                        if (PICK == KTM_PICK_LINEAR) red_shared_if(!same && !next, qc + 4u, vb);
                         va = same ? va + ca[e] : (next ? vb + ca[e] : ca[e]);
                         vb = same ? vb + cb[e] : cb[e];
                         qc = q;
