@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "ktm.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|size_t|char|unsigned\s+\w+|float|double)"
+    names = re.findall(r"^\s*(?:const\s+)?(?:void|int|size_t|char|unsigned\s+\w+|long\s+long|float|double)"
                        r"\s*\**\s*(\w+)\s*\(", src, flags=re.M)
     return sorted(set(names))
 
@@ -84,3 +84,72 @@ def test_init_three_axes_matches_reference_arithmetic(ktm_lib):
 def test_error_strings(ktm_lib):
     for code in range(8):
         assert ktm_lib.ktmGetErrorString(code)
+
+
+def test_every_export_group_is_declared():
+    names = declared_functions()
+    for n in ("ktmInterpLength", "ktmInterpTraces", "ktmSegyOpen", "ktmLoadSegySurvey",
+              "ktmReadVelModel", "ktmIBM32toIEEEDevice", "ktmReleaseMemory",
+              "ktmMigratePackedNoAlloc", "ktmLeastSquaresMigrate"):
+        assert n in names, n
+
+
+def _fake_job(ktm_lib, **over):
+    from ktm._lib import KtmJob
+    j = KtmJob()
+    ktm_lib.ktmJobInit(C.byref(j))
+    j.config.traceNo, j.config.tracePts, j.config.traceSampleRate = 4, 100, 0.004
+    j.imageX.imagePnts = j.imageY.imagePnts = 2
+    j.imageZ.imagePnts, j.imageZ.imageStep = 10, 0.004
+    for name in ("midX", "midY", "offX", "offY", "traces", "velocity", "image"):
+        setattr(j, name, 4096)     # non-NULL placeholders: every case fails before a copy
+    j.deviceMemory = 1
+    for k, v in over.items():
+        setattr(j, k, v)
+    return j
+
+
+@pytest.mark.parametrize("over", [
+    dict(weightMethod=2, pick=0),              # the fold takes the linear pick
+    dict(weightMethod=2, tracesPacked=1, traceScale=4096, traceStride=104),   # not prefolded
+    dict(traceFormat=3, tracesPacked=1),       # IBM words are raw traces
+    dict(traceFormat=3, traceScale=4096),
+    dict(weightMethod=9),
+    dict(packFormat=7),
+    dict(mode=5),
+])
+def test_job_combinations_rejected_without_device(ktm_lib, over):
+    from ktm._lib import KTM_ERR_ARG
+    j = _fake_job(ktm_lib, **over)
+    assert ktm_lib.ktmMigrate(C.byref(j)) == KTM_ERR_ARG, ktm_lib.ktmGetLastErrorMessage()
+
+
+def test_prepare_limits_without_device(ktm_lib):
+    from ktm._lib import KTM_ERR_ARG, KTM_ERR_LIMIT, KtmPrep
+    p = KtmPrep()
+    p.traceNo, p.tracePts, p.sampleRate = 4, 20000, 0.002
+    p.in_, p.out, p.outScale = 4096, 4096, 4096
+    p.rho = 3                                   # FFT of 32768 > 16384 points
+    assert ktm_lib.ktmPrepareTraces(C.byref(p)) == KTM_ERR_LIMIT
+    p.rho, p.tracePts, p.inFormat = 0, 100, 9   # not F32 or IBM-32
+    assert ktm_lib.ktmPrepareTraces(C.byref(p)) == KTM_ERR_ARG
+    p.inFormat, p.outPitch = 0, 50              # pitch < tracePts + 2
+    assert ktm_lib.ktmPrepareTraces(C.byref(p)) == KTM_ERR_ARG
+
+
+def test_interp_limits_without_device(ktm_lib):
+    from ktm._lib import KTM_ERR_ARG, KtmInterp
+    assert ktm_lib.ktmInterpLength(1001, 2) == 4001
+    assert ktm_lib.ktmInterpLength(1, 5) == 1
+    assert ktm_lib.ktmInterpLength(0, 5) == 0
+    q = KtmInterp()
+    q.traceNo, q.tracePts, q.levels, q.in_, q.out = 3, 10, 11, 4096, 4096
+    assert ktm_lib.ktmInterpTraces(C.byref(q)) == KTM_ERR_ARG        # levels > 10
+    q.levels, q.outStride = 2, 20                                    # < 37 samples
+    assert ktm_lib.ktmInterpTraces(C.byref(q)) == KTM_ERR_ARG
+
+
+def test_demigrate_pitch_rejected_without_device(ktm_lib):
+    from ktm._lib import KTM_ERR_ARG
+    j = _fake_job(ktm_lib)
+    assert ktm_lib.ktmDemigrate(C.byref(j), C.c_void_p(4096), 101) == KTM_ERR_ARG  # < nt + 2
