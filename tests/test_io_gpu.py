@@ -152,3 +152,28 @@ def test_psktm_fast_mode_rebased_utm_coordinates(cuda, ktm_lib, tmp_path):
                              oracle.ibm32_to_ieee(sv.traces), sv.velocity, pick=1, prefold=False)
     err = float(np.linalg.norm(img - ref) / np.linalg.norm(ref))
     assert err < 1e-3, err
+
+
+def test_ibm_device_all_words_exhaustive(cuda, ktm_lib):
+    """Every one of the 2^32 IBM-32 words: the device conversion is bit-identical
+    to the reference's own ktmIBM32toIEEE (compiled from its sources into
+    oracle/_ref) or, where that was not built, to the oracle restatement."""
+    import concurrent.futures as cf
+    import os as _os
+
+    import torch
+    from ktm import io as kio
+    conv = oracle.ibm32_to_ieee_reference_c if oracle.ref_available() else oracle.ibm32_to_ieee
+    n = 1 << 28
+    parts = max(1, min(32, _os.cpu_count() or 1))
+    with cf.ThreadPoolExecutor(parts) as ex:       # the C conversion releases the GIL
+        for k in range(16):
+            w64 = torch.arange(k * n, (k + 1) * n, device=cuda, dtype=torch.int64)
+            w = torch.where(w64 >= 2**31, w64 - 2**32, w64).to(torch.int32)
+            del w64
+            got = kio.ibm32_to_ieee(w).view(torch.int32).cpu().numpy()
+            words = w.cpu().numpy().view(np.uint32)
+            del w
+            ref = np.concatenate(list(ex.map(conv, np.array_split(words, parts)))).view(np.int32)
+            bad = np.flatnonzero(got != ref)
+            assert bad.size == 0, (k, hex(int(words[bad[0]])), hex(got[bad[0]]), hex(ref[bad[0]]))
