@@ -71,3 +71,28 @@ def test_config2_step_linearity_and_split(cuda, ktm_lib):
     part(slice(0, k), image=img)
     part(slice(k, None), image=img, accumulate=True)
     assert rel_l2(img.cpu().numpy(), i1.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+def test_config3_mixed_precision_whole_image(cuda, ktm_lib, fmt):
+    """Config 3: config 1 with FP16 / BF16 traces (per-trace FP32 scale), 2.5-D rho,
+    sqrt(j dt) folded in, against the FP64 device evaluation of the whole image:
+    within the 1e-3 relative L2 gate."""
+    import torch
+
+    import ktm
+    from ktm import synth
+    sv = synth.config1()
+    T = lambda x: torch.as_tensor(np.ascontiguousarray(x, dtype=np.float32)).to(cuda)  # noqa: E731
+    co = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    raw = synth.synthesize_device(sv, device=cuda, coords=co)
+    geo = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt, midX=co[0],
+               midY=co[1], offX=co[2], offY=co[3], velocity=T(sv.velocity1d),
+               aperture=sv.aperture, pick="linear")
+    p32 = ktm.prepare(raw, sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
+    nx, ny, nz = sv.shape
+    ref = ktm.migrate_columns_f64(ncols=nx * ny, traces=p32, **geo).double()
+    p = ktm.prepare(raw, sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
+    got = ktm.migrate(traces=p, **geo).reshape(nx * ny, nz).double()
+    err = float((got - ref).norm() / ref.norm())
+    assert err < 1e-3, err
