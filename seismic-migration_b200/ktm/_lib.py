@@ -208,24 +208,11 @@ def lib() -> C.CDLL:
     L.ktmInterpTraces.restype = C.c_int
     L.ktmReleaseMemory.argtypes = []
     L.ktmReleaseMemory.restype = C.c_int
-    _optional(L)
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "
                            f"binding {C.sizeof(KtmJob)} bytes")
     _lib = L
     return L
-
-
-def _optional(L) -> None:
-    """Signatures of the entry points added alongside the migration."""
-    for name, args, res in _EXTRA:
-        fn = getattr(L, name, None)
-        if fn is not None:
-            fn.argtypes = args
-            fn.restype = res
-
-
-_EXTRA: list = []
 
 
 def check(rc: int) -> None:
