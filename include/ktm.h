@@ -445,6 +445,23 @@ int ktmInterpTraces(const ktm_interp* interp);
  * the reference. */
 int ktmReleaseMemory(void);
 
+/* The fast kernels stage each chunk of packed trace rows into shared memory with
+ * one bulk (TMA) copy and wait for it with a bound of one second.  A wait that
+ * runs out ends its tile without output and is counted on the device.  This
+ * synchronises the current device and returns KTM_ERR_TIMEOUT (resetting the
+ * count) when any such wait ran out since the last check, else KTM_OK.  The
+ * synchronous entry points (host-memory ktmMigrate, ktmLeastSquaresMigrate)
+ * check by themselves; after asynchronous calls check at the caller's own
+ * synchronisation point.  No counterpart in the reference. */
+int ktmCheckDeviceWaits(void);
+
+/* Self-test of that mechanism on the current device: one CTA bulk-copies 64 KiB
+ * into shared memory and checks the bytes; with stall = 1 it first waits on a
+ * barrier that nothing arrives on, which gives up after limitMs (1..10000).
+ * Synchronous; returns ktmCheckDeviceWaits()'s status: KTM_ERR_TIMEOUT for
+ * stall = 1, KTM_OK for stall = 0. */
+int ktmSelfTestDeviceWait(int stall, int limitMs);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic data and measurement                                           */
 /* ------------------------------------------------------------------------ */

@@ -228,6 +228,16 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
                                   "(FP64 output goes through ktmMigrateColumnsF64)");
 }
 
+// KTM_ERR_TIMEOUT when a bounded device wait ran out since the last check
+int check_waits(cudaStream_t s, bool deviceSync)
+{
+    unsigned n = 0;
+    const int rc = take_wait_stalls(s, deviceSync, &n);
+    if (rc) return rc;
+    if (n) return set_error(KTM_ERR_TIMEOUT, "%u bounded device wait(s) for a bulk trace copy ran out", n);
+    return set_ok();
+}
+
 int check_job(const ktm_job* j)
 {
     if (!j) return set_error(KTM_ERR_ARG, "NULL job");
@@ -283,7 +293,7 @@ int migrate_impl(const ktm_job* j)
             KTM_CUDA_TRY(cudaMemcpyAsync(j->image, dimg, nimg * 4, cudaMemcpyDeviceToHost, s));
     }
     KTM_CUDA_TRY(cudaStreamSynchronize(s));
-    return set_ok();
+    return check_waits(s, false);
 }
 
 void dropin(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* config,
@@ -309,6 +319,23 @@ void dropin(imageGrid* imageX, imageGrid* imageY, imageGrid* imageZ, jobParams* 
 }  // namespace ktm
 
 extern "C" {
+
+int ktmCheckDeviceWaits(void)
+{
+    return ktm::check_waits(0, true);
+}
+
+int ktmSelfTestDeviceWait(int stall, int limitMs)
+{
+    if (limitMs <= 0 || limitMs > 10000) return ktm::set_error(KTM_ERR_ARG, "limitMs must be in 1..10000");
+    unsigned sum = 0;
+    int rc = ktm::wait_selftest(stall ? 1 : 0, (unsigned long long)limitMs * 1000000ull, &sum);
+    if (rc) return rc;
+    rc = ktm::check_waits(0, false);
+    if (rc) return rc;
+    if (sum != 16384u * 0x01010101u) return ktm::set_error(KTM_ERR_CUDA, "bulk copy landed wrong bytes");
+    return ktm::set_ok();
+}
 
 int ktmReleaseMemory(void)
 {

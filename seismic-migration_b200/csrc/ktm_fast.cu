@@ -46,6 +46,18 @@ constexpr int kThreads = kWarps * 32;
 constexpr size_t kFastSmemBudget = 110 * 1024;   // two CTAs per SM
 using namespace dev;
 
+// Bound of one wait for a chunk's bulk copy.  A copy of a chunk takes
+// microseconds; a wait that runs out marks the tile stalled, counts it in
+// g_waitStalls and ends the tile without output (ktmCheckDeviceWaits reports it).
+constexpr unsigned long long kBulkWaitNs = 1000000000ull;
+__device__ unsigned g_waitStalls;
+
+// Per-CTA state of the chunk pipeline: one mbarrier per trace-row buffer.
+struct ChunkSync {
+    unsigned long long bar[2];
+    int stalled;
+};
+
 struct ChunkSmem {
     // layout of one CTA's dynamic shared memory
     size_t rawBytes, crdOff, geoOff, wtabOff, total;
@@ -81,9 +93,9 @@ enum { kOutImage = 0, kOutPartial = 1, kOutAtomic = 2 };
 // run runIdx x traces [kb, ke).  Used by the grid launch (one tile per CTA) and
 // by the persistent batched launch (a queue of tiles from many jobs).
 template <int R, int PICK, int FMT, int PRE, int GRAD>
-__device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colGroup, int runIdx,
+__device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colGroup, int runIdx,
                                           int kb, int ke, float* __restrict__ partial, int outMode,
-                                          unsigned char* smem_raw, ColInfo* cinfo)
+                                          unsigned char* smem_raw, ColInfo* cinfo, ChunkSync& cs)
 {
     static_assert(R % 2 == 0, "R pairs");
     using T = typename Elem<FMT>::T;
@@ -152,8 +164,7 @@ __device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colG
         const int b = ch & 1;
         unsigned char* dst = reinterpret_cast<unsigned char*>(rawBase) + b * L.rawBytes;
         const unsigned char* src = static_cast<const unsigned char*>(a.traces) + (size_t)k0 * rowBytes;
-        const int pieces = (int)((size_t)n * rowBytes / 16);
-        for (int q = threadIdx.x; q < pieces; q += kThreads) cp_async16(dst + 16 * (size_t)q, src + 16 * (size_t)q);
+        if (threadIdx.x == 0) bulk_g2s(dst, src, (unsigned)((size_t)n * rowBytes), &cs.bar[b]);
         float* crd = crdBase + b * 5 * chunk;
         for (int q = threadIdx.x; q < 5 * n; q += kThreads) {
             const int arr = q / n, c = q % n;
@@ -169,12 +180,25 @@ __device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colG
     const f2 M2 = pk(kMagic, kMagic);
     unsigned keptTraces = 0;        // traces this warp evaluated (all lanes agree)
 
+    // thread 0 owns both barriers: it arms them, waits on them and invalidates them
+    if (threadIdx.x == 0) {
+        mbar_init(&cs.bar[0], 1);
+        mbar_init(&cs.bar[1], 1);
+        cs.stalled = 0;
+    }
     if (nchunks > 0) issue(0);
     for (int ch = 0; ch < nchunks; ch++) {
         const int b = ch & 1;
         const int k0 = kb + ch * chunk, n = min(chunk, ke - k0);
         cp_async_wait_all();
+        // the ch/2-th use of buffer b completes phase ch/2 of its barrier
+        if (threadIdx.x == 0 && !mbar_wait_bounded(&cs.bar[b], (ch >> 1) & 1, kBulkWaitNs)) {
+            cs.stalled = 1;
+            atomicAdd(&g_waitStalls, 1u);
+            mbar_wait_bounded(&cs.bar[b], (ch >> 1) & 1, kBulkWaitNs);   // the copy in flight
+        }
         __syncthreads();                       // chunk ch landed; chunk ch-1 fully consumed
+        if (cs.stalled) return false;          // CTA-uniform: no output from this tile
         if (ch + 1 < nchunks) issue(ch + 1);
         // ---- per (trace, column) distances, scale and skip flag --------------
         {
@@ -286,6 +310,10 @@ __device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colG
         }
     }
 
+    if (threadIdx.x == 0) {
+        mbar_inval(&cs.bar[0]);
+        mbar_inval(&cs.bar[1]);
+    }
     if (colValid) {
         float* out = (outMode == kOutPartial ? partial : a.image) + (size_t)col * g.nz;
 #pragma unroll
@@ -309,6 +337,7 @@ __device__ __forceinline__ void fast_tile(const FastArgs& a, int chunk, int colG
     }
     if (a.pairsEvaluated && lane == 0 && keptTraces)
         atomicAdd(a.pairsEvaluated, (unsigned long long)keptTraces * (unsigned long long)nvalid);
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -328,6 +357,7 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ColInfo cinfo[kWarps];
+    __shared__ ChunkSync cs;
     __shared__ FastArgs sa;
     __shared__ int st;
     static_assert(sizeof(FastArgs) % 4 == 0, "word copy");
@@ -341,9 +371,10 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
         int* dst = reinterpret_cast<int*>(&sa);
         for (int i = threadIdx.x; i < (int)(sizeof(FastArgs) / 4); i += kThreads) dst[i] = src[i];
         __syncthreads();
-        fast_tile<R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke, nullptr,
-                                        kOutAtomic, smem_raw, cinfo);
+        const bool ok = fast_tile<R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke,
+                                                        nullptr, kOutAtomic, smem_raw, cinfo, cs);
         __syncthreads();                           // shared memory is reused by the next tile
+        if (!ok) break;                            // CTA-uniform
     }
 }
 
@@ -353,12 +384,13 @@ fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ColInfo cinfo[kWarps];
+    __shared__ ChunkSync cs;
     const int kb = blockIdx.z * perSlice;
     const int ke = min(a.g.ntr, kb + perSlice);
     const size_t nimg = (size_t)a.g.nx * a.g.ny * a.g.nz;
     fast_tile<R, PICK, FMT, PRE, GRAD>(a, chunk, blockIdx.x, blockIdx.y, kb, ke,
                                        partial ? partial + blockIdx.z * nimg : nullptr,
-                                       partial ? kOutPartial : kOutImage, smem_raw, cinfo);
+                                       partial ? kOutPartial : kOutImage, smem_raw, cinfo, cs);
 }
 
 // out[i] = (accumulate ? out[i] : 0) + sum_z partial[z][i], z in increasing order
@@ -759,6 +791,77 @@ int launch_batch(const FastArgs* jobs, int njobs, cudaStream_t s)
         case 16: return launch_batch_r<16>(jobs, njobs, s);
         default: return set_error(KTM_ERR_ARG, "batch: tileRun must be 256, 384 or 512");
     }
+}
+
+namespace {
+
+// One CTA bulk-copies `bytes` into shared memory and sums the landed words into
+// out[0].  With stall = 1 thread 0 first waits on a second barrier that nothing
+// arrives on: the wait runs out after limitNs and is counted in g_waitStalls,
+// then the thread waits (bounded) for its own copy as a stalled tile does.
+__global__ void wait_selftest_kernel(const unsigned* __restrict__ src, unsigned bytes, int stall,
+                                     unsigned long long limitNs, unsigned* __restrict__ out)
+{
+    extern __shared__ __align__(16) unsigned char buf[];
+    __shared__ unsigned long long bar[2];
+    __shared__ int landed;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        bulk_g2s(buf, src, bytes, &bar[0]);
+        if (stall && !mbar_wait_bounded(&bar[1], 0, limitNs)) atomicAdd(&g_waitStalls, 1u);
+        landed = mbar_wait_bounded(&bar[0], 0, limitNs) ? 1 : 0;
+        if (!landed) atomicAdd(&g_waitStalls, 1u);
+        mbar_inval(&bar[0]);
+        mbar_inval(&bar[1]);
+    }
+    __syncthreads();
+    if (!landed) return;
+    const unsigned* w = reinterpret_cast<const unsigned*>(buf);
+    unsigned sum = 0;
+    for (unsigned i = threadIdx.x; i < bytes / 4; i += blockDim.x) sum += w[i];
+    atomicAdd(out, sum);
+}
+
+}  // namespace
+
+int take_wait_stalls(cudaStream_t s, bool deviceSync, unsigned* n)
+{
+    unsigned v = 0;
+    if (deviceSync) KTM_CUDA_TRY(cudaDeviceSynchronize());
+    KTM_CUDA_TRY(cudaMemcpyFromSymbolAsync(&v, g_waitStalls, sizeof(v), 0, cudaMemcpyDeviceToHost, s));
+    KTM_CUDA_TRY(cudaStreamSynchronize(s));
+    if (v) {
+        static const unsigned zero = 0;
+        KTM_CUDA_TRY(cudaMemcpyToSymbolAsync(g_waitStalls, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s));
+        KTM_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    *n = v;
+    return KTM_OK;
+}
+
+int wait_selftest(int stall, unsigned long long limitNs, unsigned* checksum)
+{
+    constexpr unsigned kBytes = 64 * 1024, kWords = kBytes / 4;
+    cudaStream_t s = 0;
+    void* mem = nullptr;
+    KTM_CUDA_TRY(pool_malloc(&mem, kBytes + 64, s));
+    unsigned* src = static_cast<unsigned*>(mem);
+    unsigned* out = src + kWords;
+    int rc = KTM_OK;
+    cudaError_t e = cudaMemsetAsync(src, 0x01, kBytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, 64, s);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(wait_selftest_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kBytes);
+    if (e == cudaSuccess) {
+        wait_selftest_kernel<<<1, 256, kBytes, s>>>(src, kBytes, stall, limitNs, out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(checksum, out, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = set_error(KTM_ERR_CUDA, "wait self-test: %s", cudaGetErrorString(e));
+    cudaFreeAsync(mem, s);
+    return rc;
 }
 
 }  // namespace ktm

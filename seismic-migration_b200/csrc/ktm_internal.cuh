@@ -72,6 +72,14 @@ int launch_fast(const FastArgs& a, cudaStream_t stream);
 // format / pick / weight; images are overwritten.
 int launch_batch(const FastArgs* jobs, int njobs, cudaStream_t s);
 
+// Bounded waits of the fast kernels (ktm_fast.cu): how many waits for a chunk's
+// bulk copy ran out (the count is reset when read).  Read on stream s after the
+// caller's work on s; deviceSync: after all work on the device.
+int take_wait_stalls(cudaStream_t s, bool deviceSync, unsigned* n);
+// One-CTA self-test of the bulk copy and its bounded wait (stall: wait first on
+// a barrier nothing arrives on); checksum = sum of the 64 KiB of 0x01 bytes landed.
+int wait_selftest(int stall, unsigned long long limitNs, unsigned* checksum);
+
 // ktm_adjoint.cu: demigration into the packed F32 layout [ntr][pitch]
 int launch_demigrate(const Geometry& g, const float* midX, const float* midY, const float* offX,
                      const float* offY, const float* vel, int velCube, const float* image,

@@ -279,6 +279,9 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
     }
     cudaError_t se = cudaStreamSynchronize(s.st);
     if (!rc && se != cudaSuccess) rc = set_error(KTM_ERR_CUDA, "lsm: %s", cudaGetErrorString(se));
+    unsigned stalls = 0;
+    if (!rc) rc = take_wait_stalls(s.st, false, &stalls);
+    if (!rc && stalls) rc = set_error(KTM_ERR_TIMEOUT, "lsm: %u bounded device wait(s) ran out", stalls);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     cudaFreeAsync(ws, s.st);

@@ -208,6 +208,10 @@ def lib() -> C.CDLL:
     L.ktmInterpTraces.restype = C.c_int
     L.ktmReleaseMemory.argtypes = []
     L.ktmReleaseMemory.restype = C.c_int
+    L.ktmCheckDeviceWaits.argtypes = []
+    L.ktmCheckDeviceWaits.restype = C.c_int
+    L.ktmSelfTestDeviceWait.argtypes = [C.c_int, C.c_int]
+    L.ktmSelfTestDeviceWait.restype = C.c_int
     if L.ktmJobStructSize() != C.sizeof(KtmJob):
         raise KtmError(-1, f"ktm_job layout mismatch: library {L.ktmJobStructSize()} bytes, "
                            f"binding {C.sizeof(KtmJob)} bytes")

@@ -90,6 +90,7 @@ def test_every_export_group_is_declared():
     names = declared_functions()
     for n in ("ktmInterpLength", "ktmInterpTraces", "ktmSegyOpen", "ktmLoadSegySurvey",
               "ktmReadVelModel", "ktmIBM32toIEEEDevice", "ktmReleaseMemory",
+              "ktmCheckDeviceWaits", "ktmSelfTestDeviceWait",
               "ktmMigratePackedNoAlloc", "ktmLeastSquaresMigrate"):
         assert n in names, n
 
