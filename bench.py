@@ -404,9 +404,9 @@ def lsm_main(a):
     kw = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt, nt=sv.nt,
               midX=coords[0], midY=coords[1], offX=coords[2], offY=coords[3],
               aperture=sv.aperture)
-    # the operator pair's weight: table (default) or sqrt.approx per pair (the fold is a
-    # migration-side preparation, not an operator weight, so it maps to the table)
-    wt = "sqrt" if a.weight == "sqrt" else "table"
+    # the operator pair's weight: prefolded (default: migration of sqrt(j dt)-folded data,
+    # demigration scaled by sqrt(j dt) per sample), the interpolated table, or sqrt.approx
+    wt = a.weight
     kw["weight"] = wt
     op = MigrationOperator(velocity=T(sv.velocity1d), **kw)
     rng = np.random.default_rng(4)

@@ -244,6 +244,9 @@ int ktmPrepareTraces(const ktm_prep* prep);
  *   data[k][j] = sum_p w(p,k) coef_j(t(p,k)/dt) m[p],   0 < j < tracePts,
  * into the packed F32 layout [traceNo][dataPitch] (dataPitch >= tracePts + 2,
  * a multiple of 4; zero guard samples), overwritten unless job->accumulate.
+ * KTM_WEIGHT_PREFOLD (linear pick): the transpose of migrating samples
+ * prefolded with sqrt(j*dt), w(p,k) = |tau_p| and every data[k][j] multiplied
+ * by sqrt(j*dt) -- no weight work per pair.
  * job->traces is not read.  Device memory, asynchronous on job->stream. */
 int ktmDemigrate(const ktm_job* job, float* data, int dataPitch);
 
@@ -259,7 +262,9 @@ int ktmVrmsGradient(const ktm_job* job, float* grad);
  * (CGLS): minimise || L m - d ||^2, L = ktmDemigrate, L^T = ktmMigrate (FAST
  * mode, packed F32 traces).  All vectors and scalars stay on the device; the
  * CG dot products and norms are FP64.  With useGraph = 1 one iteration is
- * captured in a CUDA graph and replayed. */
+ * captured in a CUDA graph and replayed.  job.weightMethod = KTM_WEIGHT_PREFOLD
+ * (linear pick) uses the prefolded operator pair: the residual is folded with
+ * sqrt(j*dt) before each migration (one more data-sized workspace vector). */
 typedef struct ktm_lsm {
     ktm_job job;                 /* geometry, coordinates, velocity, pick, aperture,
                                     weightMethod, stream; device memory */

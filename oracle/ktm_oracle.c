@@ -218,6 +218,9 @@ void oracle_demigrate_f64(const oracle_job* job, const double* image, double* da
                 }
             }
         }
+        /* prefolded weight: the migration reads sample j times sqrt(j dt) (sample_at) */
+        if (job->prefold == 1)
+            for (int j = 1; j < Nt; j++) d[j] *= sqrt((double)j * job->sampleRate);
     }
 }
 

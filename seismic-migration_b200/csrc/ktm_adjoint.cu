@@ -6,6 +6,9 @@
 // Migration (linear pick):  I[p] = |tau_p| sum_k s_k W_pk (q_k[i0] + f (q_k[i0+1] - q_k[i0]))
 // Demigration:              D_k[i0]   += W_pk |tau_p| m[p] (1 - f)
 //                           D_k[i0+1] += W_pk |tau_p| m[p] f          (0 < j < tracePts only)
+// With the prefolded weight the migration reads q_k[j] sqrt(j dt) and W_pk = 1, so the
+// demigration scatters without a weight and multiplies D_k[j] by sqrt(j dt) once per
+// sample as it writes the chunk out.
 // Every pair's (u, f, i0, W) comes from the same code as the migration's
 // (ktm_pair.cuh), so the two operators are transposes pair by pair.
 //
@@ -30,7 +33,13 @@ using namespace dev;
 constexpr int kAdjWarps = 8;
 constexpr int kAdjThreads = kAdjWarps * 32;
 constexpr int kAdjR = 16;                // tau samples per lane per run
-constexpr size_t kAdjSmemBudget = 100 * 1024;
+// Three CTAs (24 warps) per SM: the chunk's accumulators fit 72 KB and the
+// registers are capped at 80 a thread.  The scatter is latency-bound (shared
+// atomics, square roots); against two CTAs of 100 KB and 115-136 registers this
+// is 28.7 instead of 33.4 ms on the 512 x 1001 line of 32,768 traces; four CTAs
+// (64 registers) spill and take 31.9 ms.
+constexpr int kAdjMinBlocks = 3;
+constexpr size_t kAdjSmemBudget = 72 * 1024;
 
 struct AdjArgs {
     Geometry g;
@@ -68,8 +77,10 @@ __device__ __forceinline__ void red_shared_if(bool on, unsigned addr, float v)
 // starting at i = L mod 16 (slot s holds sample (s + L) mod 16), so at each step
 // the 32 lanes sit 17 samples apart and hit distinct banks; the one wrap per lane
 // is an ordinary jump.
+// WT: 0 sqrt(j dt) table interpolated per pair, 1 sqrt.approx per pair,
+//     2 prefolded (sqrt(j dt) per output sample at the write-out).
 template <int PICK, int WT>
-__global__ void __launch_bounds__(kAdjThreads)
+__global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks)
 demigrate_merge_kernel(AdjArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -159,15 +170,17 @@ demigrate_merge_kernel(AdjArgs a)
 #pragma unroll
                 for (int h = 0; h < kAdjR / 2; h++) {
                     const PairKin kk = pair_kin(DS, DR, S2[h], T2[h], umax, M2);
-                    f2 W;
+                    f2 VAL;
                     if (WT == 0) {
                         const float2 w0 = lds_f2(wS + kk.q0 * 8u), w1 = lds_f2(wS + kk.q1 * 8u);
-                        W = fma2(kk.F, pk(w0.y, w1.y), pk(w0.x, w1.x));
+                        VAL = mul2(fma2(kk.F, pk(w0.y, w1.y), pk(w0.x, w1.x)), MT[h]);
+                    } else if (WT == 1) {
+                        VAL = mul2(mul2(pk(sqrt_approx(kk.u0), sqrt_approx(kk.u1)),
+                                        pk(sqrtf(g.dt), sqrtf(g.dt))),
+                                   MT[h]);
                     } else {
-                        W = mul2(pk(sqrt_approx(kk.u0), sqrt_approx(kk.u1)),
-                                 pk(sqrtf(g.dt), sqrtf(g.dt)));
+                        VAL = MT[h];
                     }
-                    const f2 VAL = mul2(W, MT[h]);
                     float ca[2], cb[2];
                     if (PICK == KTM_PICK_LINEAR) {
                         const f2 B = mul2(VAL, kk.F);          // f * val       -> sample i0 + 1
@@ -204,7 +217,8 @@ demigrate_merge_kernel(AdjArgs a)
     __syncthreads();
     for (int i = threadIdx.x; i < n * a.pitch; i += kAdjThreads) {
         const int c = i / a.pitch, j = i % a.pitch;
-        const float v = (j > 0 && j < g.nt) ? acc[i] : 0.0f;
+        float v = (j > 0 && j < g.nt) ? acc[i] : 0.0f;
+        if (WT == 2) v *= sqrtf((float)j * g.dt);        // the fold's factor (ktm_prep.cu, ktm_lsm.cu)
         float* dst = a.data + (size_t)(k0 + c) * a.pitch + j;
         if (a.atomicOut) {
             if (v != 0.0f) atomicAdd(dst, v);
@@ -260,9 +274,13 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
         demigrate_merge_kernel<P, W><<<grid, kAdjThreads, smem, s>>>(a);                       \
     } while (0)
-    const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : 0;
+    const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : weightMethod == KTM_WEIGHT_PREFOLD ? 2 : 0;
+    if (wt == 2 && pick != KTM_PICK_LINEAR)
+        return set_error(KTM_ERR_ARG, "demigrate: the prefolded weight takes the linear pick");
     if (pick == KTM_PICK_LINEAR) {
-        if (wt) KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 1); else KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 0);
+        if (wt == 2) KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 2);
+        else if (wt) KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 1);
+        else KTM_ADJ_LAUNCH(KTM_PICK_LINEAR, 0);
     } else {
         if (wt) KTM_ADJ_LAUNCH(KTM_PICK_TRUNCATE, 1); else KTM_ADJ_LAUNCH(KTM_PICK_TRUNCATE, 0);
     }

@@ -467,8 +467,11 @@ extern "C" int ktmDemigrate(const ktm_job* job, float* data, int dataPitch)
     if (!job->deviceMemory) return set_error(KTM_ERR_ARG, "ktmDemigrate takes device memory");
     if (job->pick != KTM_PICK_TRUNCATE && job->pick != KTM_PICK_LINEAR)
         return set_error(KTM_ERR_ARG, "bad pick %d", job->pick);
-    if (job->weightMethod != KTM_WEIGHT_TABLE && job->weightMethod != KTM_WEIGHT_SQRT)
+    if (job->weightMethod != KTM_WEIGHT_TABLE && job->weightMethod != KTM_WEIGHT_SQRT &&
+        job->weightMethod != KTM_WEIGHT_PREFOLD)
         return set_error(KTM_ERR_ARG, "bad weightMethod %d", job->weightMethod);
+    if (job->weightMethod == KTM_WEIGHT_PREFOLD && job->pick != KTM_PICK_LINEAR)
+        return set_error(KTM_ERR_ARG, "the prefolded weight takes the linear pick");
     Geometry g;
     int rc = make_geometry(job, &g);
     if (rc) return rc;

@@ -98,6 +98,17 @@ __global__ void xpby(float* __restrict__ p, const float* __restrict__ s, const d
         p[i] = fmaf(b, p[i], s[i]);
 }
 
+// out[k][j] = in[k][j] sqrt(j dt) for 0 < j < nt, zero elsewhere: the prefolded
+// weight's fold, the same factor ktmPrepareTraces and the demigration apply
+__global__ void fold_samples(float* __restrict__ out, const float* __restrict__ in, int pitch, int nt,
+                             float dt, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(i % (size_t)pitch);
+        out[i] = (j > 0 && j < nt) ? in[i] * sqrtf((float)j * dt) : 0.0f;
+    }
+}
+
 // r = d - q
 __global__ void sub_into(float* __restrict__ r, const float* __restrict__ d, const float* __restrict__ q, size_t n)
 {
@@ -117,6 +128,7 @@ struct Lsm {
     int pitch;
     size_t nd, nm;              // data and model lengths
     float *r, *q, *s, *p, *ones;
+    float* rw;                  // prefolded weight: the folded residual the migration reads
     void* scratch; size_t scratchBytes; int slices;
     double *partial, *sc, *rnorm, *gnorm;
     cudaStream_t st;
@@ -128,16 +140,22 @@ struct Lsm {
         KTM_CUDA_TRY(cudaGetLastError());
         return KTM_OK;
     }
-    // data (packed F32) -> image
+    // data (packed F32) -> image; the prefolded weight folds the data first
     int migrate(const float* data, float* image)
     {
+        const bool fold = job->weightMethod == KTM_WEIGHT_PREFOLD;
+        if (fold) {
+            fold_samples<<<blocks(nd), 256, 0, st>>>(rw, data, pitch, g.nt, g.dt, nd);
+            KTM_CUDA_TRY(cudaGetLastError());
+            data = rw;
+        }
         FastArgs a;
         std::memset(&a, 0, sizeof(a));
         a.g = g;
         a.g.stride = pitch;
         a.midX = job->midX; a.midY = job->midY; a.offX = job->offX; a.offY = job->offY;
         a.traces = data; a.scale = ones; a.fmt = KTM_FMT_F32; a.pitch = pitch;
-        a.weightMode = 0; a.weightMethod = job->weightMethod;
+        a.weightMode = fold ? 2 : 0; a.weightMethod = job->weightMethod;
         a.vel = job->velocity; a.velCube = job->velocityCube;
         a.image = image; a.accumulate = 0;
         a.pick = job->pick; a.aperture = job->aperture; a.tileRun = job->tileRun;
@@ -186,8 +204,11 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
     if (L->iterations < 0) return set_error(KTM_ERR_ARG, "negative iterations");
     if (j->pick != KTM_PICK_TRUNCATE && j->pick != KTM_PICK_LINEAR)
         return set_error(KTM_ERR_ARG, "bad pick %d", j->pick);
-    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
+    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT &&
+        j->weightMethod != KTM_WEIGHT_PREFOLD)
         return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
+    if (j->weightMethod == KTM_WEIGHT_PREFOLD && j->pick != KTM_PICK_LINEAR)
+        return set_error(KTM_ERR_ARG, "the prefolded weight takes the linear pick");
     Lsm s;
     std::memset(&s, 0, sizeof(s));
     int rc = job_geometry(j, &s.g);
@@ -219,8 +240,12 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
     const int its = L->iterations;
     s.slices = (int)std::min<size_t>(64, std::max<size_t>(1, (size_t(256) << 20) / (s.nm * 4)));
     s.scratchBytes = (size_t)s.slices * s.nm * sizeof(float);
-    const size_t bytes = 2 * s.nd * 4 + 2 * s.nm * 4 + (size_t)s.g.ntr * 4 + s.scratchBytes +
-                         (kDotBlocks + kNScalars + 2 * (its + 1)) * sizeof(double) + 1024;
+    const bool fold = j->weightMethod == KTM_WEIGHT_PREFOLD;
+    // every piece starts on a 256-byte boundary (take() below)
+    auto r256 = [](size_t n) { return (n + 255) / 256 * 256; };
+    const size_t bytes = r256(kDotBlocks * sizeof(double)) + r256(kNScalars * sizeof(double)) +
+                         2 * r256((its + 1) * sizeof(double)) + (fold ? 3 : 2) * r256(s.nd * 4) +
+                         2 * r256(s.nm * 4) + r256((size_t)s.g.ntr * 4) + r256(s.scratchBytes);
     unsigned char* ws = nullptr;
     cudaError_t e = pool_malloc(reinterpret_cast<void**>(&ws), bytes, s.st);
     if (e != cudaSuccess) {
@@ -229,7 +254,7 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
                          cudaGetErrorString(e));
     }
     size_t off = 0;
-    auto take = [&](size_t n) { unsigned char* p = ws + off; off += (n + 255) / 256 * 256; return p; };
+    auto take = [&](size_t n) { unsigned char* p = ws + off; off += r256(n); return p; };
     s.partial = reinterpret_cast<double*>(take(kDotBlocks * sizeof(double)));
     s.sc = reinterpret_cast<double*>(take(kNScalars * sizeof(double)));
     s.rnorm = reinterpret_cast<double*>(take((its + 1) * sizeof(double)));
@@ -239,6 +264,7 @@ extern "C" int ktmLeastSquaresMigrate(const ktm_lsm* L)
     s.s = reinterpret_cast<float*>(take(s.nm * 4));
     s.p = reinterpret_cast<float*>(take(s.nm * 4));
     s.ones = reinterpret_cast<float*>(take((size_t)s.g.ntr * 4));
+    s.rw = fold ? reinterpret_cast<float*>(take(s.nd * 4)) : nullptr;
     s.scratch = take(s.scratchBytes);
 
     cudaGraph_t graph = nullptr;

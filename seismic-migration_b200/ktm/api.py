@@ -144,17 +144,23 @@ def packed_pitch(nt: int, fmt: str = "bf16") -> int:
 
 
 def prepare(traces, dt: float, *, fmt: str = "bf16", rho=0, prefold: bool = True,
-            script_order: bool = False, stream=None, out=None, out_scale=None) -> PackedTraces:
+            script_order: bool = False, stream=None, out=None, out_scale=None,
+            nt=None) -> PackedTraces:
     """Rho filter (ktmApplyRhoFilter.m option 1/2/3), sqrt(t) weight fold,
     per-trace scale and quantisation on the device (ktmPrepareTraces).  An
-    int32/uint32 tensor holds IBM-32 words, converted in the same pass."""
+    int32/uint32 tensor holds IBM-32 words, converted in the same pass.
+    ``nt``: the first nt samples of each row are the trace (rows of a packed
+    set, for instance); default the row length."""
     import torch
     ibm = _is_torch(traces) and traces.dtype in (torch.int32, torch.uint32)
     if not (_is_torch(traces) and traces.is_cuda and (traces.dtype == torch.float32 or ibm)):
         raise ValueError("prepare takes a CUDA float32 (or IBM-32 int32) tensor "
                          "[traceNo, tracePts]")
     traces = traces.contiguous()
-    ntr, nt = traces.shape
+    ntr, stride = traces.shape
+    nt = stride if nt is None else int(nt)
+    if not 0 < nt <= stride:
+        raise ValueError("nt must be in 1..row length")
     pitch = packed_pitch(nt, fmt)
     dtype = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[fmt]
     if out is None:
@@ -162,7 +168,7 @@ def prepare(traces, dt: float, *, fmt: str = "bf16", rho=0, prefold: bool = True
     if out_scale is None:
         out_scale = torch.empty(ntr, device=traces.device, dtype=torch.float32)
     p = _lib.KtmPrep()
-    p.traceNo, p.tracePts, p.inStride, p.sampleRate = ntr, nt, nt, float(dt)
+    p.traceNo, p.tracePts, p.inStride, p.sampleRate = ntr, nt, stride, float(dt)
     p.in_ = traces.data_ptr()
     p.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
     p.rhoScriptOrder = int(bool(script_order))

@@ -3,7 +3,10 @@
 ``MigrationOperator`` binds one survey geometry and exposes
   * ``migrate(data)``   -- L^T: packed F32 data [traceNo, pitch] -> image (ktmMigrate)
   * ``demigrate(image)`` -- L: image -> packed F32 data (ktmDemigrate)
-which are exact transposes of each other; ``Migrate`` / ``Demigrate`` wrap them
+which are exact transposes of each other (weight "table", "sqrt" or "prefold":
+with "prefold" L^T folds sqrt(j dt) into the data with ktmPrepareTraces and
+migrates the folded samples, and L scatters without a per-pair weight and
+multiplies each data sample by sqrt(j dt)); ``Migrate`` / ``Demigrate`` wrap them
 as ``torch.autograd.Function`` for the tests and the least-squares harness
 (autograd does not run inside the library).  ``vrms_gradient`` returns
 dI/dv per image sample (ktmVrmsGradient); ``least_squares`` runs CGLS on the
@@ -21,7 +24,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import KtmLsm, check, lib
-from .api import Job, PackedTraces, as_grid, packed_pitch
+from .api import Job, PackedTraces, as_grid, packed_pitch, prepare
 
 
 class MigrationOperator:
@@ -60,7 +63,12 @@ class MigrationOperator:
         import torch
         if image is None:
             image = torch.empty(self.shape, device=self.device, dtype=torch.float32)
-        return self._job(self.packed(data.contiguous()), image).run()
+        if self.weight == "prefold":
+            traces = prepare(data.contiguous(), self.dt, fmt="f32", prefold=True, nt=self.nt,
+                             stream=self.stream)
+        else:
+            traces = self.packed(data.contiguous())
+        return self._job(traces, image).run()
 
     def demigrate(self, image, data=None):
         """L m: image -> packed F32 data [traceNo, pitch]."""

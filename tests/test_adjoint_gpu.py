@@ -42,15 +42,17 @@ def line_op(dev, ncmp=48, noff=8, nt=300, nz=260, aperture=0.0, pick="linear", w
     return sv, op
 
 
-@pytest.mark.parametrize("pick", ["linear", "truncate"])
-def test_demigrate_matches_oracle_transpose(cuda, ktm_lib, pick):
+@pytest.mark.parametrize("pick,weight", [("linear", "table"), ("truncate", "table"),
+                                         ("linear", "prefold")])
+def test_demigrate_matches_oracle_transpose(cuda, ktm_lib, pick, weight):
     # truncation: a tau step incommensurate with dt (see test_parity_gpu.py)
-    sv, op = line_op(cuda, aperture=400.0, pick=pick, dtau=0.00173 if pick == "truncate" else None)
+    sv, op = line_op(cuda, aperture=400.0, pick=pick, weight=weight,
+                     dtau=0.00173 if pick == "truncate" else None)
     m = np.random.default_rng(1).standard_normal(op.shape).astype(np.float32)
     d = op.demigrate(_t(m, cuda)).cpu().numpy()
     ref = oracle.demigrate_f64(sv.imageX, sv.imageY, sv.imageZ, sv.dt, sv.midX, sv.midY, sv.offX,
                                sv.offY, sv.nt, sv.velocity, m, pick=1 if pick == "linear" else 0,
-                               aperture=400.0, prefold=3)
+                               aperture=400.0, prefold=1 if weight == "prefold" else 3)
     assert not d[:, 0].any() and not d[:, sv.nt:].any()           # guards stay zero
     # each data sample sums many FP32 contributions (5e-5); truncation: index flips
     # at FP32 rounding of t/dt move a white-noise model's contributions one sample
@@ -59,7 +61,9 @@ def test_demigrate_matches_oracle_transpose(cuda, ktm_lib, pick):
 
 
 @pytest.mark.parametrize("pick,weight,aperture", [("linear", "table", 0.0), ("linear", "table", 300.0),
-                                                  ("linear", "sqrt", 0.0), ("truncate", "table", 0.0)])
+                                                  ("linear", "sqrt", 0.0), ("truncate", "table", 0.0),
+                                                  ("linear", "prefold", 0.0),
+                                                  ("linear", "prefold", 300.0)])
 def test_dot_product(cuda, ktm_lib, pick, weight, aperture):
     import torch
     sv, op = line_op(cuda, aperture=aperture, pick=pick, weight=weight)
@@ -73,10 +77,11 @@ def test_dot_product(cuda, ktm_lib, pick, weight, aperture):
     assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
 
 
-def test_dot_product_adjoint_config(cuda, ktm_lib):
+@pytest.mark.parametrize("weight", ["table", "prefold"])
+def test_dot_product_adjoint_config(cuda, ktm_lib, weight):
     """512 CMPs x 64 offsets x 1001 samples at 4 ms, seeded Gaussian model and data."""
     import torch
-    sv, op = line_op(cuda, ncmp=512, noff=64, nt=1001, nz=1001, seed=4)
+    sv, op = line_op(cuda, ncmp=512, noff=64, nt=1001, nz=1001, seed=4, weight=weight)
     rng = np.random.default_rng(11)
     m = _t(rng.standard_normal(op.shape), cuda)
     d = op.pack(_t(rng.standard_normal((op.ntr, sv.nt)), cuda))
@@ -132,10 +137,10 @@ def test_vrms_gradient_central_differences(cuda, ktm_lib):
     assert ktm is not None
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_least_squares_migration(cuda, ktm_lib, use_graph):
+@pytest.mark.parametrize("use_graph,weight", [(True, "table"), (False, "table"), (True, "prefold")])
+def test_least_squares_migration(cuda, ktm_lib, use_graph, weight):
     import torch
-    sv, op = line_op(cuda, ncmp=128, noff=16, nt=501, nz=501, seed=9)
+    sv, op = line_op(cuda, ncmp=128, noff=16, nt=501, nz=501, seed=9, weight=weight)
     rng = np.random.default_rng(2)
     m_true = np.where(rng.uniform(size=op.shape) < 0.05, rng.standard_normal(op.shape), 0.0)
     d = op.demigrate(_t(m_true, cuda))

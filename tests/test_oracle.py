@@ -93,11 +93,11 @@ def test_f64_adjoint_dot_product():
     vel = np.linspace(1500, 2500, 60).astype(np.float32)
     d = rng.standard_normal((ntr, nt)).astype(np.float32)
     m = rng.standard_normal((6, 2, 60))
-    for pick in (0, 1):
+    for pick, prefold in ((0, 0), (1, 0), (1, 1), (1, 3)):
         Ld = oracle.migrate_f64(gx, gy, gz, 0.004, mid[:, 0], mid[:, 1], off[:, 0], off[:, 1], d,
-                                vel, pick=pick, aperture=120.0)
+                                vel, pick=pick, aperture=120.0, prefold=prefold)
         Ltm = oracle.demigrate_f64(gx, gy, gz, 0.004, mid[:, 0], mid[:, 1], off[:, 0], off[:, 1], nt,
-                                   vel, m, pick=pick, aperture=120.0)
+                                   vel, m, pick=pick, aperture=120.0, prefold=prefold)
         lhs, rhs = np.vdot(Ld, m), np.vdot(d.astype(np.float64), Ltm)
         assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0)
 
