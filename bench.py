@@ -370,6 +370,9 @@ def line_main(a):
     if not a.no_cpu_baseline:
         r, cores, kind, sample = cpu_reference_rate(sv, a.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        if kind == "reference" and cores > 1:
+            r1, _, _, s1 = cpu_reference_rate(sv, a.cpu_seconds / 3, 1)
+            cpu["one_thread"] = {"value": r1 / 1e9, "sample": s1}
     print(json.dumps({
         "metric": METRIC, "value": out["f16"]["gpair_s"], "unit": UNIT, "n_gpus": 1,
         "steps": a.steps, "higher_is_better": True, "dtype": "f16 traces, f32 accumulate",
@@ -686,6 +689,11 @@ def main():
         sub = synth.config2(ntr=4096, seed=2)
         r, cores, kind, sample = cpu_reference_rate(sub, a.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        if kind == "reference" and cores > 1:
+            # the one-thread run of the same code (the configuration reference mode matches
+            # bit for bit; the OpenMP loop races on image[] with more threads)
+            r1, _, _, s1 = cpu_reference_rate(sub, a.cpu_seconds / 3, 1)
+            cpu["one_thread"] = {"value": r1 / 1e9, "sample": s1}
 
     # DRAM bytes of one step from the ncu capture summarised in profiles/ (one step of
     # the same workload), scaled to this batch by its traces

@@ -14,7 +14,9 @@ any exchange in the data path:
 
 For a small image with very many traces the alternative is to shard the
 traces and sum the images once (``migrate_trace_shard``: one ``all_reduce``
-or ``reduce`` of the FP32 image).
+or ``reduce`` of the FP32 image).  Least-squares migration shards the same way
+(``least_squares_trace_shard``: per CGLS iteration one ``all_reduce`` of the
+image and two of an FP64 scalar).
 
 The migration itself is a callable (``ktm.migrate`` by default) so that the
 partitioning and the collectives can be exercised on CPU ranks (gloo).
@@ -179,3 +181,59 @@ def migrate_trace_shard(*, midX, midY, offX, offY, traces, group=None, dst: int 
         return t
     dist.reduce(t, dst=dst, op=dist.ReduceOp.SUM, group=group)
     return t if rank == dst else None
+
+
+def least_squares_trace_shard(migrate, demigrate, data, model, iterations: int, group=None):
+    """Least-squares migration (CGLS, as ktmLeastSquaresMigrate) with the traces
+    sharded over the ranks of ``group``: rank k holds its data shard d_k and
+    L = [L_0; L_1; ...] stacks the ranks' demigrations, so
+
+        L p   = (L_k p) on each rank, no exchange;
+        L^T r = sum_k L_k^T r_k: one all_reduce of the image;
+        <q, q>, <r, r> = sums over ranks: all_reduce of one FP64 scalar each.
+
+    ``migrate(r_k)`` returns L_k^T r_k (an image tensor), ``demigrate(p)`` returns
+    L_k p (a data tensor shaped like ``data``).  ``model`` is the starting model,
+    the same on every rank; it is updated in place and returned with the residual
+    norms ||d - L m_i|| and gradient norms ||L^T (d - L m_i)|| (float64 arrays of
+    iterations + 1).  Every rank takes the same collectives in the same order;
+    without an initialised process group the ranks are one (no collective).
+    Vectors keep the dtype and device of ``data`` / ``model``; dot products are
+    FP64."""
+    import torch
+    import torch.distributed as dist
+    sharded = dist.is_available() and dist.is_initialized()
+
+    def allsum(t):
+        if sharded:
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t
+
+    def dot(x, y):
+        return torch.dot(x.reshape(-1).double(), y.reshape(-1).double())
+
+    def scalar_sum(x):
+        return float(allsum(x.reshape(1).clone())[0])
+
+    r = data - demigrate(model)
+    s = allsum(migrate(r))
+    p = s.clone()
+    gamma = float(dot(s, s))
+    rn = np.zeros(iterations + 1)
+    gn = np.zeros(iterations + 1)
+    rn[0] = np.sqrt(scalar_sum(dot(r, r)))
+    gn[0] = np.sqrt(gamma)
+    for it in range(1, iterations + 1):
+        q = demigrate(p)
+        delta = scalar_sum(dot(q, q))
+        alpha = gamma / delta if delta > 0.0 else 0.0
+        model += alpha * p
+        r -= alpha * q
+        s = allsum(migrate(r))
+        gamma_new = float(dot(s, s))
+        beta = gamma_new / gamma if gamma > 0.0 else 0.0
+        gamma = gamma_new
+        p = s + beta * p
+        rn[it] = np.sqrt(scalar_sum(dot(r, r)))
+        gn[it] = np.sqrt(gamma)
+    return model, rn, gn

@@ -180,3 +180,20 @@ def test_autograd_wrappers(cuda, ktm_lib):
     expect = op.migrate(op.demigrate(m.detach()) - d_obs)
     # demigration accumulates with shared-memory atomics: sums agree to FP32 rounding
     assert rel_l2(m.grad.cpu().numpy(), expect.cpu().numpy()) < 1e-5
+
+
+def test_trace_sharded_cgls_on_one_rank_matches_library(cuda, ktm_lib):
+    """ktm.shard.least_squares_trace_shard (the CGLS that shards traces over
+    ranks; here one rank, no process group) with the CUDA operator pair takes
+    the same steps as ktmLeastSquaresMigrate."""
+    import torch
+    from ktm import shard
+    sv, op = line_op(cuda, ncmp=64, noff=8, nt=300, nz=300, seed=12, weight="prefold")
+    rng = np.random.default_rng(3)
+    m_true = np.where(rng.uniform(size=op.shape) < 0.05, rng.standard_normal(op.shape), 0.0)
+    d = op.demigrate(_t(m_true, cuda))
+    a, rna, gna = op.least_squares(d, 8, use_graph=True)
+    b, rnb, gnb = shard.least_squares_trace_shard(op.migrate, op.demigrate, d.clone(),
+                                                  torch.zeros(op.shape, device=cuda), 8)
+    assert np.allclose(rna, rnb, rtol=1e-3) and np.allclose(gna, gnb, rtol=1e-3)
+    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-3
