@@ -43,7 +43,12 @@ namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr size_t kFastSmemBudget = 110 * 1024;   // two CTAs per SM
+// Three CTAs (24 warps) per SM: 74 KB of dynamic shared memory each (3 x (74 KB +
+// static + 1 KB reserved) fits the SM's 228 KB) and registers capped at 80.  Against
+// two CTAs of 110 KB and 128 registers: 426 instead of 455 ms per 16,384 FP16
+// traces on the 200 x 200 x 1501 image; four CTAs (64 registers) take 478 ms.
+constexpr int kFastMinBlocks = 3;
+constexpr size_t kFastSmemBudget = 74 * 1024;
 using namespace dev;
 
 // Bound of one wait for a chunk's bulk copy.  A copy of a chunk takes
@@ -351,7 +356,7 @@ struct BatchTile {
 };
 
 template <int R, int PICK, int FMT, int PRE>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kFastMinBlocks)
 batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
              const BatchTile* __restrict__ tiles, int ntiles, unsigned* __restrict__ counter)
 {
@@ -379,7 +384,7 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
 }
 
 template <int R, int PICK, int FMT, int PRE, int GRAD>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kFastMinBlocks)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -424,8 +429,8 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
     const unsigned gx = (unsigned)((cols + kWarps - 1) / kWarps);
     const unsigned gy = (unsigned)((g.nz + 32 * R - 1) / (32 * R));
     if (gy > 65535) return set_error(KTM_ERR_LIMIT, "fast kernel: Nz too large");
-    // trace slices: enough CTAs for about four waves of two CTAs per SM, each
-    // slice keeping at least four chunks of traces
+    // trace slices: about eight CTAs per SM (close to three waves of three resident
+    // CTAs), each slice keeping at least four chunks of traces
     const long long base = (long long)gx * gy;
     const long long want = 8LL * smCount;
     int slices = (int)((want + base - 1) / base);
@@ -649,7 +654,7 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
     int dev = 0, sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
-    const int ctas = 2 * sm;
+    const int ctas = kFastMinBlocks * sm;
     std::vector<int> chunks(njobs);
     size_t smem = 0;
     double totalPairs = 0.0;
