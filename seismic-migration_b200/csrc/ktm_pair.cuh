@@ -151,11 +151,6 @@ __device__ __forceinline__ unsigned smem_u32(const void* p)
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
 {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
