@@ -1,8 +1,9 @@
 // ktm_pair.cuh -- device helpers shared by the gather kernels (migration,
 // demigration, velocity gradient): packed f32x2 arithmetic, the special-function
 // square root, shared-memory sample loads through 32-bit addresses, cp.async and
-// bulk (TMA) copies with bounded mbarrier waits, and the per-pair kinematics, so that every operator evaluates the same
-// traveltime, sample index, fraction and weight bit for bit.
+// bulk (TMA) copies with bounded mbarrier waits, and the per-pair kinematics, so
+// that every operator evaluates the same traveltime, sample index, fraction and
+// weight bit for bit.
 #pragma once
 
 #include "ktm_internal.cuh"
