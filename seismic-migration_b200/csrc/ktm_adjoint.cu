@@ -40,6 +40,8 @@ constexpr int kAdjR = 16;                // tau samples per lane per run
 // (64 registers) spill and take 31.9 ms.
 constexpr int kAdjMinBlocks = 3;
 constexpr size_t kAdjSmemBudget = 72 * 1024;
+static_assert(kAdjMinBlocks * (kAdjSmemBudget + 1024) <= 228 * 1024,
+              "three CTAs must fit the SM's 228 KB of shared memory");
 
 struct AdjArgs {
     Geometry g;

@@ -49,6 +49,10 @@ constexpr int kThreads = kWarps * 32;
 // traces on the 200 x 200 x 1501 image; four CTAs (64 registers) take 478 ms.
 constexpr int kFastMinBlocks = 3;
 constexpr size_t kFastSmemBudget = 74 * 1024;
+// per CTA: the dynamic budget, up to 1 KB of static shared memory (ColInfo,
+// ChunkSync, the batch kernel's FastArgs) and the 1 KB the SM reserves
+static_assert(kFastMinBlocks * (kFastSmemBudget + 2048) <= 228 * 1024,
+              "three CTAs must fit the SM's 228 KB of shared memory");
 using namespace dev;
 
 // Bound of one wait for a chunk's bulk copy.  A copy of a chunk takes
@@ -62,6 +66,8 @@ struct ChunkSync {
     unsigned long long bar[2];
     int stalled;
 };
+static_assert(sizeof(ColInfo) * kWarps + sizeof(ChunkSync) + sizeof(FastArgs) + sizeof(int) <= 1024,
+              "static shared memory of the fast kernels within the 1 KB allowance");
 
 struct ChunkSmem {
     // layout of one CTA's dynamic shared memory
