@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--lsm-jobs", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=None,
+                    help="--impl reference: CPU seconds per step (default: about 150 s "
+                         "spread over warm-up and timed steps, at least 2 s each)")
     ap.add_argument("--tile-run", type=int, default=0,
                     help="tau samples per warp run: 256, 384 or 512 (0: chosen by Nz)")
     ap.add_argument("--weight", default="prefold", choices=["prefold", "table", "sqrt"],
@@ -174,7 +177,8 @@ def reference_arm(a):
     sv = synth.config2(ntr=20000)
     threads = os.cpu_count() or 1
     rates = []
-    budget = max(2.0, 150.0 / max(1, a.steps + a.warmup))
+    budget = (a.ref_step_seconds if a.ref_step_seconds is not None
+              else max(2.0, 150.0 / max(1, a.steps + a.warmup)))
     info = None
     for i in range(a.warmup + a.steps):
         r, cores, kind, sample = cpu_reference_rate(sv, budget, threads)

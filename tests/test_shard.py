@@ -202,3 +202,19 @@ def test_least_squares_trace_sharding_gloo(tmp_path):
         z = np.load(tmp_path / f"lsm{k}.npz")
         assert np.allclose(z["rn"], rn, rtol=1e-9) and np.allclose(z["gn"], gn, rtol=1e-9)
         assert np.allclose(z["m"], m.numpy(), rtol=1e-8, atol=1e-10 * np.abs(m.numpy()).max())
+
+
+def test_least_squares_trace_shard_solves_a_dense_system():
+    """The CGLS of least_squares_trace_shard on one rank with dense operators
+    (L = A, L^T = A^T): it reaches the least-squares solution of an
+    overdetermined system, and ||r|| never increases."""
+    import torch
+    rng = np.random.default_rng(21)
+    A = torch.from_numpy(rng.standard_normal((60, 14)))
+    b = torch.from_numpy(rng.standard_normal(60))
+    x, rn, gn = shard.least_squares_trace_shard(lambda r: A.T @ r, lambda m: A @ m, b.clone(),
+                                                torch.zeros(14, dtype=torch.float64), 40)
+    ref = np.linalg.lstsq(A.numpy(), b.numpy(), rcond=None)[0]
+    assert np.allclose(x.numpy(), ref, rtol=1e-8, atol=1e-10)
+    assert np.all(np.diff(rn) <= 1e-12 * rn[0])
+    assert gn[-1] < 1e-8 * gn[0]
