@@ -11,7 +11,7 @@
  *     reference run with one OpenMP thread.  Pinned by the golden fixtures in
  *     tests/golden/ that the reference's own code produced.
  *   - oracle_migrate_f64 / oracle_demigrate_f64 / oracle_vrms_grad_f64: the same
- *     method in FP64, extended with the north-star features the reference lacks
+ *     method in FP64, extended with the features the fast kernels add and the reference lacks
  *     (linear trace interpolation, aperture, laterally varying Vrms cube).  With
  *     pick = truncate, no aperture and a 1-D velocity it is psktmCPU.c in FP64.
  */

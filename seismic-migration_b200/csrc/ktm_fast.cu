@@ -1,7 +1,8 @@
 // ktm_fast.cu -- the fast PSTM gather kernel (mixed precision) and the FP64
 // device reference.
 //
-// Method (psktmCPU.c:56-86, extended as the north star asks):
+// Method (psktmCPU.c:56-86, extended with linear pick, aperture, a Vrms cube and
+// packed FP16 / BF16 / FP32 samples with a per-trace scale):
 //   image[x,tau] = |tau| * sum_k  s_k * w(t) * pick(q_k, t/dt)
 //   t = sqrt(tau^2 + |s-x|^2 S) + sqrt(tau^2 + |r-x|^2 S),  S = 1/v(x,tau)^2
 //   reference weight t*sqrt(tau^2/t) = |tau| sqrt(t) (:85): |tau| per image
