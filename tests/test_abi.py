@@ -154,3 +154,38 @@ def test_demigrate_pitch_rejected_without_device(ktm_lib):
     from ktm._lib import KTM_ERR_ARG
     j = _fake_job(ktm_lib)
     assert ktm_lib.ktmDemigrate(C.byref(j), C.c_void_p(4096), 101) == KTM_ERR_ARG  # < nt + 2
+
+
+def test_header_compiles_as_c_and_cpp_and_links(tmp_path, ktm_lib):
+    """A C caller of the reference's kind: include/ktm.h compiles as C11 and C++17,
+    and a program using the drop-in's host helpers links against libktm.so and runs
+    without a GPU."""
+    import shutil
+    import subprocess
+    import ktm
+    if shutil.which("gcc") is None or shutil.which("g++") is None:
+        pytest.skip("no host compiler")
+    inc = os.path.join(ROOT, "include")
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "ktm.h"\n'
+        "int main(void) {\n"
+        "  struct imageGrid gx = {3, 12.5f, 100.0f}, gy = {2, 25.0f, 0.0f}, gz = {4, 0.002f, 0.0f};\n"
+        "  float xx[3], yy[2], zz[4];\n"
+        "  initThreeAxes(&gx, &gy, &gz, xx, yy, zz);\n"
+        '  printf("%.4f %.4f %.4f %s\\n", xx[2], yy[1], zz[3], ktmGetErrorString(KTM_ERR_LIMIT));\n'
+        "  return 0;\n}\n")
+    for cc, std, name in (("gcc", "-std=c11", "c"), ("g++", "-std=c++17", "cpp")):
+        r = subprocess.run([cc, std, "-Wall", "-Werror", "-fsyntax-only", "-x",
+                            "c" if name == "c" else "c++", "-I" + inc, str(src)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    libdir = os.path.dirname(ktm.LIB_PATH)
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c11", "-I" + inc, str(src), "-o", str(exe), "-L" + libdir, "-lktm",
+                        "-Wl,-rpath," + libdir], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    x, y, z, msg = r.stdout.split(" ", 3)
+    assert (float(x), float(y), float(z)) == (125.0, 25.0, 0.006) and msg.strip()
