@@ -75,14 +75,17 @@ struct ChunkSmem {
     size_t rawBytes, crdOff, geoOff, wtabOff, total;
 };
 
-__host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize, int nt)
+// table: the kernel interpolates sqrt(j dt) from a per-CTA table (the table weight);
+// the prefolded and sqrt.approx weights need none, and their chunks grow by its size
+__host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize, int nt,
+                                                           bool table)
 {
     ChunkSmem L;
     L.rawBytes = (size_t)chunk * pitch * esize;              // one buffer
     L.crdOff = 2 * L.rawBytes;                               // [2][5][chunk] floats
     L.geoOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
     L.wtabOff = L.geoOff + (size_t)chunk * kWarps * sizeof(float4);
-    L.total = L.wtabOff + (size_t)(nt + 1) * sizeof(float2);   // [nt+1] weight table
+    L.total = L.wtabOff + (table ? (size_t)(nt + 1) * sizeof(float2) : 0);   // [nt+1] weight table
     return L;
 }
 
@@ -112,7 +115,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
     static_assert(R % 2 == 0, "R pairs");
     using T = typename Elem<FMT>::T;
     const Geometry& g = a.g;
-    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt);
+    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt, PRE == kWtTable);
     T* rawBase = reinterpret_cast<T*>(smem_raw);
     float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
     float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
@@ -424,11 +427,12 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
     const Geometry& g = a.g;
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
     int chunk = 32;
-    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize, g.nt).total > kFastSmemBudget) chunk--;
-    if (chunk_layout(chunk, a.pitch, esize, g.nt).total > (size_t)kMaxSmemBytes)
+    constexpr bool kTable = PRE == kWtTable;
+    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total > kFastSmemBudget) chunk--;
+    if (chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total > (size_t)kMaxSmemBytes)
         return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
                                         "stage limit", a.pitch);
-    const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt).total;
+    const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total;
     auto kern = fast_kernel<R, PICK, FMT, PRE, GRAD>;
     KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
@@ -668,8 +672,9 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
     for (int j = 0; j < njobs; j++) {
         const Geometry& g = jobs[j].g;
         int c = 32;
-        while (c > 1 && chunk_layout(c, jobs[j].pitch, esize, g.nt).total > kFastSmemBudget) c--;
-        const size_t need = chunk_layout(c, jobs[j].pitch, esize, g.nt).total;
+        while (c > 1 && chunk_layout(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total > kFastSmemBudget)
+            c--;
+        const size_t need = chunk_layout(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total;
         if (need > (size_t)kMaxSmemBytes)
             return set_error(KTM_ERR_LIMIT, "batch: job %d packed pitch %d exceeds shared memory", j,
                              jobs[j].pitch);
