@@ -308,11 +308,20 @@ int ktmAutotune(const ktm_job* job, int* tileRun);
  *     (4 Mi floats) that each GPU loading the library keeps until exit.
  *   - Limit: images of at most 2 Mi samples (Nx*Ny*Nz <= 2097152); larger
  *     images are rejected with KTM_ERR_LIMIT.
+ *   - Accepts what ktmMigrateBatch accepts for one job: F32 / F16 / BF16 packed
+ *     samples, linear or truncating pick, KTM_WEIGHT_TABLE / _SQRT, and
+ *     KTM_WEIGHT_PREFOLD with samples prepared with prefold = 1; accumulate.
  *   - The first call on a device looks up that device's copy of the array
- *     (with the device current); make that first call before any stream capture.
+ *     (with the device current).  Under CUDA's lazy module loading (the
+ *     default) that first call also loads the module holding the array, which
+ *     creates it on the device: a one-time implicit allocation that may
+ *     synchronise.  Make that first call during set-up, before any stream
+ *     capture.
  *   - Every call uses the same array: calls that overlap on the GPU (other
  *     streams, other host threads on the same device) race.  Nothing in the
- *     array has to start at zero; each call overwrites what it reads. */
+ *     array has to start at zero; each call writes every partial image before
+ *     it reads it.  After KTM_ERR_TIMEOUT from ktmCheckDeviceWaits the image
+ *     of the call concerned is undefined (a tile that gave up wrote nothing). */
 int ktmMigratePackedNoAlloc(const ktm_job* job);
 
 /* FP64 device evaluation of the job's method (pick, aperture, Vrms cube,
@@ -450,11 +459,21 @@ int ktmInterpTraces(const ktm_interp* interp);
  * the reference. */
 int ktmReleaseMemory(void);
 
+/* Counters of that memory pool: *allocations = stream-ordered allocations the
+ * library has made since it was loaded (all devices); *reservedBytes /
+ * *usedBytes = the current device's pool, reserved and in use (0 when the
+ * library has not allocated on it).  Any pointer may be NULL.  No counterpart
+ * in the reference. */
+int ktmMemoryStats(unsigned long long* allocations, size_t* reservedBytes, size_t* usedBytes);
+
 /* The fast kernels stage each chunk of packed trace rows into shared memory with
  * one bulk (TMA) copy and wait for it with a bound of one second.  A wait that
  * runs out ends its tile without output and is counted on the device.  This
  * synchronises the current device and returns KTM_ERR_TIMEOUT (resetting the
  * count) when any such wait ran out since the last check, else KTM_OK.  The
+ * images of the calls since the last check are then undefined: a tile that
+ * gave up contributed nothing, and where the launch sums trace slices, the
+ * slice it left unwritten holds stale values.  The
  * synchronous entry points (host-memory ktmMigrate, ktmLeastSquaresMigrate)
  * check by themselves; after asynchronous calls check at the caller's own
  * synchronisation point.  No counterpart in the reference. */

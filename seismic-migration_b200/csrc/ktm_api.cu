@@ -3,6 +3,7 @@
 #include "ktm_internal.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 #include <map>
@@ -38,10 +39,12 @@ constexpr int kPoolDevices = 64;
 std::mutex g_poolMu;
 cudaMemPool_t g_pool[kPoolDevices];
 bool g_poolTried[kPoolDevices];
+std::atomic<unsigned long long> g_poolCalls{0};   // pool_malloc calls since the library loaded
 }  // namespace
 
 cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s)
 {
+    g_poolCalls.fetch_add(1, std::memory_order_relaxed);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -356,6 +359,35 @@ int ktmReleaseMemory(void)
     return ktm::set_ok();
 }
 
+int ktmMemoryStats(unsigned long long* allocations, size_t* reservedBytes, size_t* usedBytes)
+{
+    if (allocations) *allocations = ktm::g_poolCalls.load(std::memory_order_relaxed);
+    int dev = 0;
+    if (reservedBytes) *reservedBytes = 0;
+    if (usedBytes) *usedBytes = 0;
+    if (!reservedBytes && !usedBytes) return ktm::set_ok();
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return ktm::set_error(KTM_ERR_CUDA, "ktmMemoryStats: %s", cudaGetErrorString(e));
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(ktm::g_poolMu);
+        if (dev >= 0 && dev < ktm::kPoolDevices) pool = ktm::g_pool[dev];
+    }
+    if (!pool) return ktm::set_ok();                 // nothing allocated on this device yet
+    uint64_t v = 0;
+    if (reservedBytes) {
+        e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v);
+        if (e != cudaSuccess) return ktm::set_error(KTM_ERR_CUDA, "ktmMemoryStats: %s", cudaGetErrorString(e));
+        *reservedBytes = (size_t)v;
+    }
+    if (usedBytes) {
+        e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v);
+        if (e != cudaSuccess) return ktm::set_error(KTM_ERR_CUDA, "ktmMemoryStats: %s", cudaGetErrorString(e));
+        *usedBytes = (size_t)v;
+    }
+    return ktm::set_ok();
+}
+
 // status hooks of the host-side file I/O (ktm_io.c)
 int ktm_io_error(int code, const char* msg) { return ktm::set_error(code, "%s", msg); }
 int ktm_io_ok(void) { return ktm::set_ok(); }
@@ -516,7 +548,6 @@ extern "C" int ktmVrmsGradient(const ktm_job* job, float* grad)
 }
 
 namespace ktm {
-namespace {
 
 // FastArgs of a device-memory FAST job on a packed trace set.
 int packed_args(const ktm_job* j, FastArgs* a)
@@ -545,6 +576,8 @@ int packed_args(const ktm_job* j, FastArgs* a)
     a->pairsEvaluated = j->pairsEvaluated;
     return KTM_OK;
 }
+
+namespace {
 
 struct TuneKey {
     int nx, ny, nz, nt, fmt, pick, weightMode, weightMethod;

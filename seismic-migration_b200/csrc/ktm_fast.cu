@@ -22,18 +22,22 @@
 //   u   = min(u, nt)   (also maps NaN to nt, a zero guard)
 //   i0  = floor(u) via the round-down add of 1.5*2^23, f = u - i0
 //   v   = q[i0] + f (q[i0+1] - q[i0]);  acc += s_k * v
-// Work decomposition (148 SMs, two 8-warp CTAs per SM):
+// Work decomposition (148 SMs, three 8-warp CTAs per SM, 80 registers and 74 KB
+// of dynamic shared memory each):
 //   warp   = one image column x a run of 32*R tau samples (lane L owns
 //            tau = run0 + L + 32 r): a warp reads a narrow window of a trace;
 //   CTA    = 8 columns (blockIdx.x) x one run (blockIdx.y) x one slice of the
 //            traces (blockIdx.z); slices write partial images that a second
 //            kernel sums in a fixed order (deterministic), so small images still
 //            fill the GPU;
-//   traces stream through shared memory in chunks, double-buffered with
-//   16-byte cp.async; for each chunk the CTA first computes per (trace,
-//   column) the squared distances and a skip flag (aperture, or a lower bound
-//   of u over the run beyond the trace end), so the inner loop branches once
-//   per trace, warp-uniformly.
+//   traces stream through shared memory in chunks, double-buffered: thread 0
+//   moves a chunk's packed rows (one contiguous, 16-byte aligned range) with a
+//   single bulk copy (cp.async.bulk) completed on the buffer's mbarrier, waited
+//   for with a one-second bound; the coordinates and scales follow in 4-byte
+//   cp.async.  For each chunk the CTA first computes per (trace, column) the
+//   squared distances and a skip flag (aperture, or a lower bound of u over the
+//   run beyond the trace end), so the inner loop branches once per trace,
+//   warp-uniformly.
 #include "ktm_pair.cuh"
 
 #include <algorithm>

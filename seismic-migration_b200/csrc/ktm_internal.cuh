@@ -94,6 +94,9 @@ cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t s);
 
 // ktm_api.cu: geometry of a job (validates sizes)
 int job_geometry(const ktm_job* j, Geometry* g);
+// ktm_api.cu: FastArgs of a device-memory FAST job on a packed trace set (checks the
+// job; KTM_WEIGHT_PREFOLD needs tracesPrefolded and becomes weightMode 2)
+int packed_args(const ktm_job* j, FastArgs* a);
 
 // ktm_prep.cu
 int packed_pitch(int nt, int fmt);

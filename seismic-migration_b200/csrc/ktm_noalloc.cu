@@ -10,10 +10,12 @@
 // library keeps until the process exits.  Host code only ever sees the array's
 // host-side stand-in symbol; its device address is looked up once per device
 // with cudaGetSymbolAddress, with that device current, on the first call made
-// on that device.
+// on that device.  With CUDA's lazy module loading (the default) that lookup is
+// also what loads this file's module, which creates the array on the device:
+// a one-time implicit allocation at the first call per device, so that call
+// belongs in the caller's set-up.
 #include "ktm_internal.cuh"
 
-#include <cstring>
 #include <mutex>
 
 namespace ktm {
@@ -58,54 +60,24 @@ extern "C" int ktmMigratePackedNoAlloc(const ktm_job* j)
 {
     using namespace ktm;
     if (!j) return set_error(KTM_ERR_ARG, "NULL job");
-    if (!j->deviceMemory)
-        return set_error(KTM_ERR_ARG, "ktmMigratePackedNoAlloc takes device memory only");
-    if (j->mode != KTM_MODE_FAST || !j->tracesPacked)
-        return set_error(KTM_ERR_ARG, "ktmMigratePackedNoAlloc takes FAST mode and a packed trace "
-                                      "set (ktmPrepareTraces)");
-    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_BF16)
-        return set_error(KTM_ERR_ARG, "bad traceFormat %d", j->traceFormat);
-    if (j->pick != KTM_PICK_TRUNCATE && j->pick != KTM_PICK_LINEAR)
-        return set_error(KTM_ERR_ARG, "bad pick %d", j->pick);
-    if (j->weightMethod != KTM_WEIGHT_TABLE && j->weightMethod != KTM_WEIGHT_SQRT)
-        return set_error(KTM_ERR_ARG, "bad weightMethod %d", j->weightMethod);
-    if (j->imageX.imagePnts < 0 || j->imageY.imagePnts < 0 || j->imageZ.imagePnts < 0 ||
-        j->config.traceNo < 0 || j->config.tracePts < 0 || !(j->config.traceSampleRate > 0.0f))
-        return set_error(KTM_ERR_ARG, "bad sizes or sample rate");
-    const size_t nimg = (size_t)j->imageX.imagePnts * j->imageY.imagePnts * j->imageZ.imagePnts;
+    if (!j->deviceMemory || j->mode != KTM_MODE_FAST || !j->tracesPacked)
+        return set_error(KTM_ERR_ARG, "ktmMigratePackedNoAlloc takes FAST mode, device memory and a "
+                                      "packed trace set (ktmPrepareTraces)");
+    // the same checks and arguments as the batched and tuned launches of packed sets
+    // (KTM_WEIGHT_PREFOLD with prefolded samples included)
+    FastArgs a;
+    int rc = packed_args(j, &a);
+    if (rc) return rc;
+    const size_t nimg = (size_t)a.g.nx * a.g.ny * a.g.nz;
     if (nimg > kNoAllocMaxImage)
         return set_error(KTM_ERR_LIMIT,
                          "ktmMigratePackedNoAlloc: image of %zu samples exceeds the limit of %zu "
                          "(static scratch of %zu floats holds at least two partial images)",
                          nimg, kNoAllocMaxImage, kNoAllocScratchFloats);
-    if (j->config.traceNo > 0 && (!j->midX || !j->midY || !j->offX || !j->offY || !j->traces ||
-                                  !j->traceScale))
-        return set_error(KTM_ERR_ARG, "NULL coordinate, trace or scale pointer");
-    if (nimg > 0 && (!j->image || !j->velocity)) return set_error(KTM_ERR_ARG, "NULL image or velocity");
 
     void* scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
+    rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
-
-    FastArgs a;
-    std::memset(&a, 0, sizeof(a));
-    Geometry& g = a.g;
-    g.nx = j->imageX.imagePnts; g.ny = j->imageY.imagePnts; g.nz = j->imageZ.imagePnts;
-    g.x0 = j->imageX.imageStart; g.dx = j->imageX.imageStep;
-    g.y0 = j->imageY.imageStart; g.dy = j->imageY.imageStep;
-    g.z0 = j->imageZ.imageStart; g.dz = j->imageZ.imageStep;
-    g.ntr = j->config.traceNo; g.nt = j->config.tracePts;
-    g.stride = j->traceStride > 0 ? j->traceStride : j->config.tracePts;
-    g.dt = j->config.traceSampleRate;
-    a.midX = j->midX; a.midY = j->midY; a.offX = j->offX; a.offY = j->offY;
-    a.traces = j->traces; a.scale = j->traceScale; a.fmt = j->traceFormat; a.pitch = g.stride;
-    a.weightMode = j->tracesPrefolded ? 2 : 0;
-    a.weightMethod = j->weightMethod;
-    a.vel = j->velocity; a.velCube = j->velocityCube;
-    a.image = j->image; a.accumulate = j->accumulate;
-    a.pick = j->pick; a.aperture = j->aperture;
-    a.tileRun = j->tileRun;
-    a.pairsEvaluated = j->pairsEvaluated;
     // every partial image is written completely before the ordered sum reads it,
     // so nothing in the shared array needs clearing between calls
     a.scratch = scratch;

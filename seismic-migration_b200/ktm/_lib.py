@@ -208,6 +208,9 @@ def lib() -> C.CDLL:
     L.ktmInterpTraces.restype = C.c_int
     L.ktmReleaseMemory.argtypes = []
     L.ktmReleaseMemory.restype = C.c_int
+    L.ktmMemoryStats.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_size_t),
+                                 C.POINTER(C.c_size_t)]
+    L.ktmMemoryStats.restype = C.c_int
     L.ktmCheckDeviceWaits.argtypes = []
     L.ktmCheckDeviceWaits.restype = C.c_int
     L.ktmSelfTestDeviceWait.argtypes = [C.c_int, C.c_int]
@@ -224,6 +227,14 @@ def check(rc: int) -> None:
         L = lib()
         raise KtmError(rc, L.ktmGetLastErrorMessage().decode(errors="replace")
                        or L.ktmGetErrorString(rc).decode())
+
+
+def memory_stats() -> dict:
+    """The library's own device memory pool (ktmMemoryStats): allocations made
+    since it loaded, and the current device's reserved / used bytes."""
+    n, r, u = C.c_ulonglong(), C.c_size_t(), C.c_size_t()
+    check(lib().ktmMemoryStats(C.byref(n), C.byref(r), C.byref(u)))
+    return {"allocations": int(n.value), "reserved": int(r.value), "used": int(u.value)}
 
 
 def last_error() -> tuple[int, str]:

@@ -89,7 +89,7 @@ def test_error_strings(ktm_lib):
 def test_every_export_group_is_declared():
     names = declared_functions()
     for n in ("ktmInterpLength", "ktmInterpTraces", "ktmSegyOpen", "ktmLoadSegySurvey",
-              "ktmReadVelModel", "ktmIBM32toIEEEDevice", "ktmReleaseMemory",
+              "ktmReadVelModel", "ktmIBM32toIEEEDevice", "ktmReleaseMemory", "ktmMemoryStats",
               "ktmCheckDeviceWaits", "ktmSelfTestDeviceWait",
               "ktmMigratePackedNoAlloc", "ktmLeastSquaresMigrate"):
         assert n in names, n
@@ -189,3 +189,11 @@ def test_header_compiles_as_c_and_cpp_and_links(tmp_path, ktm_lib):
     assert r.returncode == 0, r.stderr
     x, y, z, msg = r.stdout.split(" ", 3)
     assert (float(x), float(y), float(z)) == (125.0, 25.0, 0.006) and msg.strip()
+
+
+def test_memory_stats_counter_without_device(ktm_lib):
+    """The allocation counter is host state: readable without a GPU (and no call
+    on the CPU has allocated)."""
+    n = C.c_ulonglong(123)
+    assert ktm_lib.ktmMemoryStats(C.byref(n), None, None) == 0
+    assert n.value == 0
