@@ -45,6 +45,15 @@ METRIC = "PSTM G(image-pt x trace)/s on 1 B200: mixed vs plain FP32 @<=1e-3 rel 
 UNIT = "Gpair/s"
 WORKLOAD = "3D PSTM 200x200x1501 image, 1e6 traces x 1501 samples @ 2 ms, aperture 3 km"
 
+# DRAM read + write of the migration kernel per trace of a step on the full 200 x 200 x
+# 1501 image (FP16 packed traces, five launches of 40 MB trace blocks per 62,500-trace
+# step): 3.76 GB per step from one ncu capture of a full bench step
+# (profiles/migrate_fast_3d-62500-traces_dram-traffic.md), divided by its traces.
+MIGRATE_DRAM_BYTES_PER_TRACE = 3.76e9 / 62500
+MIGRATE_DRAM_NOTE = ("DRAM read+write per step from one ncu capture of a full step (5 launches "
+                     "of the kernel, one per 40 MB trace block), scaled by the traces of the "
+                     "step; measured on the whole image (N=1)")
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -57,7 +66,8 @@ def parse():
     ap.add_argument("--fmt", default="f16", choices=["f16", "bf16", "f32"])
     ap.add_argument("--err-side", type=int, default=64,
                     help="error check on a seeded random SIDE x SIDE x Nz subgrid (FP64 device)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="steps of the end-to-end measurement (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--skip-error", action="store_true", help="skip the FP64 error check")
@@ -65,7 +75,12 @@ def parse():
                     help="3d: the headline workload; batch: 64 target-oriented jobs in one "
                          "persistent launch")
     ap.add_argument("--jobs", type=int, default=64)
-    ap.add_argument("--lsm-jobs", type=int, default=4)
+    ap.add_argument("--lsm-jobs", type=int, default=None,
+                    help="--config batch: jobs that run 10 CGLS iterations (default: all)")
+    ap.add_argument("--batch-fmt", default="both", choices=["f16", "bf16", "both"],
+                    help="--config batch: trace formats to time (both: FP16 first, BF16 beside)")
+    ap.add_argument("--err-cols", type=int, default=64,
+                    help="--config batch: sampled columns per job for the error")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=None,
                     help="--impl reference: CPU seconds per step (default: about 150 s "
@@ -132,40 +147,65 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------------------
-def cpu_reference_rate(sv, seconds: float, threads: int):
+class CpuReference:
     """The reference's psktmCPU.c (oracle/_ref, compiled unmodified) or, where it
     was never built, the oracle's single-thread restatement, on a bounded sample
-    of the workload: the full image against the first T traces, T sized so the
-    run takes about ``seconds``.  Returns (pairs/s, cores, kind, sample)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    kind = "reference" if oracle.ref_available() else "port"
-    if kind == "port":
-        threads = 1
-    nx, ny, nz = sv.shape
+    of the workload: the full image against the first T traces.
 
-    def run(ntr):
-        tr = np.random.default_rng(5).standard_normal((ntr, sv.nt)).astype(np.float32)
-        args = (sv.imageX, sv.imageY, sv.imageZ, sv.dt, sv.midX[:ntr], sv.midY[:ntr],
-                sv.offX[:ntr], sv.offY[:ntr], tr, sv.velocity1d)
+    psktmCPU.c spreads its trace loop over the OpenMP threads (psktmCPU.c:56-59),
+    so T is sized from a probe that gives every thread two traces, then rounded
+    up to a multiple of the thread count with at least eight traces per thread,
+    so that no thread idles in a last partial wave."""
+
+    def __init__(self, sv, seconds: float, threads: int):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        self.oracle = oracle
+        self.kind = "reference" if oracle.ref_available() else "port"
+        self.threads = threads if self.kind == "reference" else 1
+        g = oracle.grid
+        self.grids = tuple(g(x.imagePnts, x.imageStep, x.imageStart)
+                           for x in (sv.imageX, sv.imageY, sv.imageZ))
+        self.sv = sv
+        self.npts = int(np.prod(sv.shape))
+        self.tr = np.random.default_rng(5).standard_normal((sv.ntr, sv.nt)).astype(np.float32)
+        th = self.threads
+        probe = min(sv.ntr, 2 * th)
+        rate = probe / self.run(probe)                     # traces per second, all threads
+        t = int(seconds * rate)
+        t = max(t, 8 * th)
+        t = -(-t // th) * th                               # whole waves of the thread team
+        self.ntr = max(1, min(sv.ntr, t))
+
+    def run(self, ntr: int) -> float:
+        sv = self.sv
+        args = (*self.grids, sv.dt, sv.midX[:ntr], sv.midY[:ntr], sv.offX[:ntr],
+                sv.offY[:ntr], self.tr[:ntr], sv.velocity1d)
         t0 = time.perf_counter()
-        if kind == "reference":
-            oracle.migrate_reference_c(*args, threads=threads)
+        if self.kind == "reference":
+            self.oracle.migrate_reference_c(*args, threads=self.threads)
         else:
-            oracle.migrate_ref32(*args)
+            self.oracle.migrate_ref32(*args)
         return time.perf_counter() - t0
 
-    g = oracle.grid
-    sv.imageX, sv.imageY, sv.imageZ = (g(a.imagePnts, a.imageStep, a.imageStart)
-                                       for a in (sv.imageX, sv.imageY, sv.imageZ))
-    t1 = run(1)
-    ntr = int(max(1, min(sv.ntr, seconds / max(t1, 1e-3))))
-    dt = run(ntr)
-    pairs = nx * ny * nz * ntr
-    sample = (f"full {nx}x{ny}x{nz} image x first {ntr} traces ({pairs:.3e} pairs), "
-              f"1-D RMS velocity, {threads} OpenMP threads" if kind == "reference" else
-              f"full image x first {ntr} traces, single-thread oracle restatement")
-    return pairs / dt, threads, kind, sample
+    def rate(self) -> float:
+        """pairs/s of one timed run of the sized sample."""
+        return self.npts * self.ntr / self.run(self.ntr)
+
+    def sample(self) -> str:
+        nx, ny, nz = self.sv.shape
+        pairs = self.npts * self.ntr
+        if self.kind == "reference":
+            return (f"full {nx}x{ny}x{nz} image x first {self.ntr} traces ({pairs:.3e} pairs, "
+                    f"{self.ntr // self.threads} per thread), 1-D RMS velocity, "
+                    f"{self.threads} OpenMP threads")
+        return f"full image x first {self.ntr} traces, single-thread oracle restatement"
+
+
+def cpu_reference_rate(sv, seconds: float, threads: int):
+    """(pairs/s, cores, kind, sample) of the reference CPU code on a sized sample."""
+    ref = CpuReference(sv, seconds, threads)
+    return ref.rate(), ref.threads, ref.kind, ref.sample()
 
 
 def reference_arm(a):
@@ -176,25 +216,49 @@ def reference_arm(a):
     from ktm import synth
     sv = synth.config2(ntr=20000)
     threads = os.cpu_count() or 1
-    rates = []
     budget = (a.ref_step_seconds if a.ref_step_seconds is not None
               else max(2.0, 150.0 / max(1, a.steps + a.warmup)))
-    info = None
+    ref = CpuReference(sv, budget, threads)
+    rates = []
     for i in range(a.warmup + a.steps):
-        r, cores, kind, sample = cpu_reference_rate(sv, budget, threads)
+        r = ref.rate()
         if i >= a.warmup:
             rates.append(r)
-        info = (cores, kind, sample)
     v = float(np.mean(rates)) / 1e9
-    cores, kind, sample = info
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "per_step": "bounded CPU sample, see cpu_baseline"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+                         "sample": ref.sample()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def rho_filter_f64(traces, dt: float, opt: int):
+    """FP64 rho filter of ktmApplyRhoFilter.m:22-62, trace by trace, on the traces'
+    device: zero padding to M = 2^ceil(log2 m), omega_k = 2 pi k / dt for the FFT's
+    k = -M/2 .. M/2-1 (the script's scaling, no 1/M), 2D |omega|, 2.5D
+    sqrt|omega| exp(i pi/4 sign omega), 3D i omega; the real part of the inverse
+    FFT, truncated to m samples.  The first stage of the FP64 pipeline the bench's
+    image error is measured against; returns float64 [n, m]."""
+    import math
+
+    import torch
+    x = traces.double()
+    m = x.shape[1]
+    M = 1 << (m - 1).bit_length() if m > 1 else 1
+    F = torch.fft.fft(x, n=M, dim=1)
+    k = torch.fft.fftfreq(M, d=1.0 / M, device=x.device, dtype=torch.float64)
+    omega = 2.0 * math.pi * k / float(dt)
+    if opt == 1:
+        H = omega.abs().to(torch.complex128)
+    elif opt == 2:
+        H = omega.abs().sqrt() * torch.exp(1j * (math.pi / 4.0) * torch.sign(omega))
+    else:
+        H = 1j * omega
+    return torch.fft.ifft(F * H[None, :], dim=1).real[:, :m].contiguous()
 
 
 # ---------------------------------------------------------------------------------------
@@ -205,11 +269,13 @@ def batch_main(a):
     4 ms); trace counts log-uniform in [1e4, 5e5]; per job, sources and receivers
     uniform over the patch grown by the 2 km aperture, offsets <= 3150 m, the
     line survey's Vrms(t0) = 1500 + 0.5 t0[ms], 25 Hz Ricker diffractions from
-    20 scatterers plus sigma 0.05 noise, 2.5-D rho filter, BF16 traces with an
-    FP32 scale and sqrt(j dt) folded in, FP32 accumulation, tau-run length from
-    ktmAutotune.  Then the
-    error of sampled jobs against the FP64 device evaluation, and 10-iteration
-    CGLS (one iteration captured in a CUDA graph) on the smallest jobs."""
+    20 scatterers plus sigma 0.05 noise, 2.5-D rho filter, sqrt(j dt) folded in,
+    a per-trace FP32 scale, FP32 accumulation, tile shape from ktmAutotune.
+
+    Each trace format (FP16 by default, BF16 beside it) is timed as one launch over
+    all jobs; every job's error is measured against an FP64 pipeline from its raw
+    traces (FP64 rho filter, FP64 migration) on sampled columns; then 10 CGLS
+    iterations (one iteration captured in a CUDA graph and replayed) per job."""
     import torch
 
     import ktm
@@ -219,7 +285,8 @@ def batch_main(a):
     torch.cuda.set_device(dev)
     rng = np.random.default_rng(55)
     T = lambda x: torch.as_tensor(np.ascontiguousarray(x, dtype=np.float32)).to(dev)  # noqa: E731
-    jobs, surveys = [], []
+    fmts = ["f16", "bf16"] if a.batch_fmt == "both" else [a.batch_fmt]
+    geos, packs, surveys = [], {f: [] for f in fmts}, []
     t0 = time.perf_counter()
     for j in range(a.jobs):
         side = int(round(np.exp(rng.uniform(np.log(16), np.log(128)))))
@@ -233,67 +300,93 @@ def batch_main(a):
         sv.imageX.imageStart = sv.imageY.imageStart = 2000.0 + 6.25
         coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
         raw = synth.synthesize_device(sv, device=dev, coords=coords)
-        packed = ktm.prepare(raw, sv.dt, fmt="bf16", rho=sv.rho_opt, prefold=True)
+        for f in fmts:
+            packs[f].append(ktm.prepare(raw, sv.dt, fmt=f, rho=sv.rho_opt, prefold=True))
         del raw
-        jobs.append(dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+        geos.append(dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
                          midX=coords[0], midY=coords[1], offX=coords[2], offY=coords[3],
-                         traces=packed, velocity=T(sv.velocity1d), pick="linear",
-                         aperture=sv.aperture,
-                         image=torch.empty(sv.shape, device=dev, dtype=torch.float32)))
+                         velocity=T(sv.velocity1d), pick="linear", aperture=sv.aperture))
         surveys.append(sv)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
-    run = ktm.autotune(**jobs[0])
-    for kw in jobs:
-        kw["tile_run"] = run
     pairs = sum(s.pairs for s in surveys)
-    ktm.migrate_batch(jobs)                                   # warm-up
-    torch.cuda.synchronize()
-    times = []
-    for _ in range(max(1, a.steps)):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        ktm.migrate_batch(jobs)
-        e1.record()
+    runs, images = {}, {}
+    for f in fmts:
+        imgs = [torch.empty(s.shape, device=dev, dtype=torch.float32) for s in surveys]
+        jobs = [dict(g, traces=p, image=im) for g, p, im in zip(geos, packs[f], imgs)]
+        tune = ktm.autotune(**jobs[int(np.argmax([s.pairs for s in surveys]))])
+        for kw in jobs:
+            kw["tile_run"] = tune
+        ktm.migrate_batch(jobs)                               # warm-up
         torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-    ms = float(np.median(times))
-    # per-job error on sampled jobs and columns
-    errs = []
-    for j in rng.choice(len(jobs), size=min(8, len(jobs)), replace=False):
-        sv, kw = surveys[j], jobs[j]
-        raw = synth.synthesize_device(sv, device=dev, coords=[kw[k] for k in ("midX", "midY", "offX", "offY")])
-        p32 = ktm.prepare(raw, sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
-        del raw
+        times = []
+        for _ in range(max(1, a.steps)):
+            e0, e1 = _events()
+            e0.record()
+            ktm.migrate_batch(jobs)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = float(np.median(times))
+        runs[f] = {"value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_launch": ms,
+                   "launches": len(times), "tile_run": tune}
+        images[f] = imgs
+    # every job's error against the FP64 pipeline from its raw traces, on sampled columns
+    per_job = []
+    for j, (sv, g) in enumerate(zip(surveys, geos)):
+        raw = synth.synthesize_device(sv, device=dev, coords=[g[k] for k in ("midX", "midY", "offX", "offY")])
         nx, ny, nz = sv.shape
-        cols = torch.as_tensor(rng.choice(nx * ny, size=min(32, nx * ny), replace=False).astype(np.int32))
-        ref = ktm.migrate_columns_f64(columns=cols, **{**kw, "traces": p32, "image": None,
-                                                       "tile_run": 0}).double()
-        got = kw["image"].reshape(nx * ny, nz)[cols.to(dev).long()].double()
-        errs.append(float((got - ref).norm() / ref.norm()))
-    # 10-iteration CGLS per job (graph-captured iteration) on the smallest jobs
+        cols = torch.as_tensor(np.sort(rng.choice(nx * ny, size=min(a.err_cols, nx * ny),
+                                                  replace=False)).astype(np.int32))
+        f64 = rho_filter_f64(raw, sv.dt, sv.rho_opt)
+        ref = ktm.migrate_columns_f64(columns=cols, traces=f64, **g).double()
+        del f64, raw
+        row = {"job": j, "side": nx, "traces": sv.ntr, "columns": int(cols.numel())}
+        for f in fmts:
+            got = images[f][j].reshape(nx * ny, nz)[cols.to(dev).long()].double()
+            row[f] = float((got - ref).norm() / ref.norm())
+        per_job.append(row)
+    errors = {}
+    for f in fmts:
+        e = np.array([r[f] for r in per_job])
+        errors[f] = {"max": float(e.max()), "median": float(np.median(e)), "jobs": len(e),
+                     "over_1e-3": int((e > 1e-3).sum())}
+    # 10-iteration CGLS per job (one iteration graph-captured), on the job's rho-filtered data
     lsm = []
-    for j in np.argsort([s.pairs for s in surveys])[: a.lsm_jobs]:
-        sv, kw = surveys[j], jobs[j]
+    nlsm = len(surveys) if a.lsm_jobs is None else min(a.lsm_jobs, len(surveys))
+    order = np.argsort([s.pairs for s in surveys])[:nlsm]
+    t_all = time.perf_counter()
+    for j in sorted(order):
+        sv, g = surveys[j], geos[j]
         op = MigrationOperator(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
-                               nt=sv.nt, midX=kw["midX"], midY=kw["midY"], offX=kw["offX"],
-                               offY=kw["offY"], velocity=kw["velocity"], aperture=sv.aperture)
-        d = op.pack(kw["traces"].unpacked())
+                               nt=sv.nt, midX=g["midX"], midY=g["midY"], offX=g["offX"],
+                               offY=g["offY"], velocity=g["velocity"], aperture=sv.aperture)
+        raw = synth.synthesize_device(sv, device=dev, coords=[g[k] for k in ("midX", "midY", "offX", "offY")])
+        d = op.pack(ktm.prepare(raw, sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False).unpacked())
+        del raw
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         _, rn, _ = op.least_squares(d, 10, use_graph=True)
-        lsm.append({"job": int(j), "traces": sv.ntr, "image": list(sv.shape),
+        lsm.append({"job": int(j), "traces": sv.ntr, "side": sv.shape[0],
                     "residual_ratio": float(rn[-1] / rn[0]), "seconds": time.perf_counter() - t1})
+        del d
+    lsm_s = time.perf_counter() - t_all
+    main_fmt = fmts[0]
     print(json.dumps({
-        "metric": METRIC, "config": {"workload": f"batched: {len(jobs)} jobs in one persistent launch",
+        "metric": METRIC, "config": {"workload": f"batched: {len(surveys)} jobs in one persistent launch",
                                      "patch_sides": [s.shape[0] for s in surveys],
                                      "traces": [s.ntr for s in surveys], "nz": 751,
-                                     "trace_format": "bf16", "tile_run": run,
+                                     "trace_format": main_fmt,
                                      "weight": "sqrt(j dt) folded into the packed samples"},
-        "value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_launch": ms, "pairs": pairs,
-        "steps": len(times), "error_rel_l2": {"max": max(errs), "median": float(np.median(errs)),
-                                               "jobs": len(errs), "vs": "FP64 device, 32 columns per job"},
-        "lsm_10_iterations": lsm, "setup_s": setup_s,
+        "value": runs[main_fmt]["value"], "unit": UNIT, "pairs": pairs, "formats": runs,
+        "error_rel_l2": errors,
+        "error_vs": ("FP64 pipeline from each job's raw traces: FP64 rho filter (2.5-D), then FP64 "
+                     f"migration (|tau| sqrt(t) per pair); {a.err_cols} sampled columns per job"),
+        "per_job": per_job,
+        "lsm_10_iterations": {"jobs": len(lsm), "seconds_total": lsm_s,
+                              "residual_ratio_max": max((r["residual_ratio"] for r in lsm), default=None),
+                              "per_job": lsm},
+        "setup_s": setup_s,
     }), flush=True)
 
 
@@ -486,7 +579,7 @@ def main():
     import torch
 
     import ktm
-    from ktm import synth
+    from ktm import shard, synth
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -501,51 +594,89 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    # ---- workload: each rank images its own 5 x 5 km tile (weak scaling, no data-path
-    # collective); rank r's survey is the same recipe with seed 2 + r
+    def allmax(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # ---- workload: ONE survey; its 200 x 200 image is cut into one output tile per
+    # rank (shard.tile_partition) and each rank keeps the traces whose midpoints lie
+    # within the aperture of its tile (shard.select_traces, FP64 on the host).  No
+    # collective touches the data path; tiles stay on their ranks.
     t_setup = time.perf_counter()
-    sv = synth.config2(ntr=a.ntr, seed=2 + rank)
+    sv = synth.config2(ntr=a.ntr, seed=2)
+    tiles = shard.tile_partition(sv.shape[0], sv.shape[1], world)
+    tile = tiles[rank]
+    idx = shard.select_traces(sv.midX, sv.midY, tile, sv.imageX, sv.imageY, sv.aperture)
+    gx, gy = tile.grids(sv.imageX, sv.imageY)
     T = lambda x: torch.as_tensor(np.ascontiguousarray(x)).to(dev)  # noqa: E731
-    coords = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
-    vel = T(sv.velocity)
+    coords_all = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    idx_d = torch.as_tensor(idx.astype(np.int64), device=dev)
+    coords = [c.index_select(0, idx_d).contiguous() for c in coords_all]
+    vel = shard.tile_velocity(T(sv.velocity), tile)
     vel1 = T(sv.velocity1d)
-    raw = torch.empty((sv.ntr, sv.nt), device=dev, dtype=torch.float32)
+    raw = torch.empty((len(idx), sv.nt), device=dev, dtype=torch.float32)
     chunk = 100_000
     for k0 in range(0, sv.ntr, chunk):
-        synth.synthesize_device(sv, k0, min(sv.ntr, k0 + chunk), device=dev, coords=coords,
-                                out=raw[k0:min(sv.ntr, k0 + chunk)])
+        k1 = min(sv.ntr, k0 + chunk)
+        lo, hi = (int(v) for v in np.searchsorted(idx, [k0, k1]))
+        if hi > lo:
+            blk = synth.synthesize_device(sv, k0, k1, device=dev, coords=coords_all)
+            raw[lo:hi] = blk.index_select(0, idx_d[lo:hi] - k0)
+            del blk
+    del coords_all
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
 
+    # a step = one batch of the survey's traces (1/16 by default); this rank takes the
+    # batch's traces it selected, which are contiguous in its arrays (idx is sorted)
     nb = a.batches
     bsz = (sv.ntr + nb - 1) // nb
-    bounds = [(b * bsz, min(sv.ntr, (b + 1) * bsz)) for b in range(nb)]
+    sbounds = [(b * bsz, min(sv.ntr, (b + 1) * bsz)) for b in range(nb)]
+    bounds = [tuple(int(v) for v in np.searchsorted(idx, [b0, b1])) for b0, b1 in sbounds]
     nx, ny, nz = sv.shape
-    npts = nx * ny * nz
+    npts = nx * ny * nz                      # the whole image: pairs count the job's work
+    tnx, tny = tile.shape
+    tpts = tnx * tny * nz
     stream = torch.cuda.Stream(device=dev)
-    image = torch.zeros(sv.shape, device=dev, dtype=torch.float32)
+    image = torch.zeros((tnx, tny, nz), device=dev, dtype=torch.float32)
     pitch = ktm.packed_pitch(sv.nt, a.fmt)
     tdtype = {"f16": torch.float16, "bf16": torch.bfloat16, "f32": torch.float32}[a.fmt]
-    pbuf = torch.empty((bsz, pitch), device=dev, dtype=tdtype)
-    pscale = torch.empty(bsz, device=dev, dtype=torch.float32)
+    maxb = max(1, max(k1 - k0 for k0, k1 in bounds))
+    pbuf = torch.empty((maxb, pitch), device=dev, dtype=tdtype)
+    pscale = torch.empty(maxb, device=dev, dtype=torch.float32)
     counter = torch.zeros(1, device=dev, dtype=torch.int64)
+    geo = dict(imageX=gx, imageY=gy, imageZ=sv.imageZ, dt=sv.dt, pick="linear",
+               aperture=sv.aperture)
 
     def step(i, count=False):
         k0, k1 = bounds[i % nb]
         n = k1 - k0
         with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            if n == 0:
+                e0.record(stream)
+                e1.record(stream)
+                return e0, e1, n
             p = ktm.prepare(raw[k0:k1], sv.dt, fmt=a.fmt, rho=sv.rho_opt,
                             prefold=a.weight == "prefold",
                             stream=stream, out=pbuf[:n], out_scale=pscale[:n])
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            ktm.migrate(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
-                        midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
+            ktm.migrate(midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
                         offY=coords[3][k0:k1], traces=p, velocity=vel, image=image,
-                        pick="linear", aperture=sv.aperture, accumulate=(i > 0), stream=stream,
+                        accumulate=(i > 0), stream=stream,
                         pairs_counter=counter if count else None, weight=a.weight,
-                        tile_run=a.tile_run)
+                        tile_run=a.tile_run, **geo)
             e1.record(stream)
         return e0, e1, n
 
@@ -566,36 +697,34 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     counter.zero_()
     ev0.record(stream)
-    kev, traces_done = [], 0
+    kev, traces_done, survey_traces = [], 0, 0
     for i in range(a.steps):
         # the counter costs one atomic add per warp at kernel exit
         e0, e1, n = step(i, count=True)
         kev.append((e0, e1))
         traces_done += n
+        b0, b1 = sbounds[i % nb]
+        survey_traces += b1 - b0
     ev1.record(stream)
     stream.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    ms_rank = ev0.elapsed_time(ev1)
     kernel_ms = sum(e0.elapsed_time(e1) for e0, e1 in kev)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    pairs_rank = npts * traces_done
-    value = pairs_rank * world / (ms * 1e-3) / 1e9
+    ms = allmax(ms_rank)
+    job_pairs = npts * survey_traces          # the whole image against every trace of the steps
+    value = job_pairs / (ms * 1e-3) / 1e9
 
     # evaluated pairs (after aperture / end-of-trace culling), counted by the kernel
     evaluated = int(counter.item())
     sfu_rate = evaluated * 2 / (kernel_ms * 1e-3)      # two sqrt.approx per evaluated pair
     # in-aperture pairs of the timed batches, counted independently of the kernel
-    # (|mid - x| <= aperture over all image columns, in FP64; times Nz)
+    # (|mid - x| <= aperture over the tile's columns, in FP64; times Nz)
     in_aperture = 0
-    cx = (sv.imageX.imageStart + sv.imageX.imageStep *
-          torch.arange(nx, device=dev, dtype=torch.float64)).repeat_interleave(ny)
-    cy = (sv.imageY.imageStart + sv.imageY.imageStep *
-          torch.arange(ny, device=dev, dtype=torch.float64)).repeat(nx)
+    cx = (gx.imageStart + gx.imageStep *
+          torch.arange(tnx, device=dev, dtype=torch.float64)).repeat_interleave(tny)
+    cy = (gy.imageStart + gy.imageStep *
+          torch.arange(tny, device=dev, dtype=torch.float64)).repeat(tnx)
     for i in range(a.steps):
         k0, k1 = bounds[i % nb]
         for j0 in range(k0, k1, 4096):
@@ -603,44 +732,68 @@ def main():
             dx = coords[0][j0:j1, None].double() - cx[None, :]
             dy = coords[1][j0:j1, None].double() - cy[None, :]
             in_aperture += int(((dx * dx + dy * dy) <= sv.aperture ** 2).sum().item()) * nz
+    # per-rank balance: traces kept, pairs evaluated, device time
+    stats = torch.tensor([len(idx), evaluated, ms_rank, kernel_ms], device=dev, dtype=torch.float64)
+    if dist:
+        allstats = [torch.empty_like(stats) for _ in range(world)]
+        dist.all_gather(allstats, stats)
+    else:
+        allstats = [stats]
+    per_rank = [{"rank": r, "tile": [tiles[r].ix0, tiles[r].ix1, tiles[r].iy0, tiles[r].iy1],
+                 "traces": int(st[0]), "evaluated_pairs": int(st[1]), "ms": float(st[2]),
+                 "kernel_ms": float(st[3])}
+                for r, st in enumerate(t.cpu().tolist() for t in allstats)]
+    evaluated_all = sum(r["evaluated_pairs"] for r in per_rank)
+    in_aperture_all = int(allsum(float(in_aperture)))
 
-    # ---- accuracy: one batch, fresh image, vs FP64 device evaluation (rho-filtered
-    # FP32 input, weight |tau| sqrt(t) per pair) on sampled columns
-    rel_l2 = max_err = None
-    ncols_err = (0, 0)
+    # ---- accuracy: one batch through the product path (device rho filter, FP16 packing,
+    # fast kernel) into a fresh image, against an FP64 pipeline from the same raw traces:
+    # the FP64 rho filter (ktmApplyRhoFilter.m) then the FP64 migration with the weight
+    # |tau| sqrt(t) per pair, on a seeded random subgrid of the rank's tile.  Beside it,
+    # the kernel alone: the FP64 migration of the FP32 traces the device filter produced.
+    err = None
     if not a.skip_error:
         k0, k1 = bounds[0]
         image_keep = image.clone()
         image.zero_()
         step(0)
         stream.synchronize()
+        rng = np.random.default_rng(17 + rank)
+        xs = np.sort(rng.choice(tnx, size=min(a.err_side, tnx), replace=False))
+        ys = np.sort(rng.choice(tny, size=min(a.err_side, tny), replace=False))
+        cols = torch.as_tensor((xs[:, None] * tny + ys[None, :]).ravel().astype(np.int32))
+        got = image.reshape(tnx * tny, nz)[cols.to(dev).long()].double()
+        egeo = dict(columns=cols, midX=coords[0][k0:k1], midY=coords[1][k0:k1],
+                    offX=coords[2][k0:k1], offY=coords[3][k0:k1], velocity=vel, **geo)
+        f64 = rho_filter_f64(raw[k0:k1], sv.dt, sv.rho_opt)
+        ref = ktm.migrate_columns_f64(traces=f64, **egeo).double()
+        del f64
         p32 = ktm.prepare(raw[k0:k1], sv.dt, fmt="f32", rho=sv.rho_opt, prefold=False)
-        rng = np.random.default_rng(17)
-        xs = np.sort(rng.choice(nx, size=min(a.err_side, nx), replace=False))
-        ys = np.sort(rng.choice(ny, size=min(a.err_side, ny), replace=False))
-        cols = torch.as_tensor((xs[:, None] * ny + ys[None, :]).ravel().astype(np.int32))
-        ncols_err = (len(xs), len(ys))
-        ref = ktm.migrate_columns_f64(
-            columns=cols, imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
-            midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
-            offY=coords[3][k0:k1], traces=p32, velocity=vel, pick="linear", aperture=sv.aperture)
-        # p32 is not prefolded: the FP64 evaluation applies |tau| sqrt(t) per pair
-        got = image.reshape(nx * ny, nz)[cols.to(dev).long()].double()
-        ref = ref.double()
-        rel_l2 = float((got - ref).norm() / ref.norm())
-        max_err = float((got - ref).abs().max() / ref.abs().max())
+        ref_k = ktm.migrate_columns_f64(traces=p32, **egeo).double()
         del p32
+        err = {"rel_l2": allmax(float((got - ref).norm() / ref.norm())),
+               "max_rel": allmax(float((got - ref).abs().max() / ref.abs().max())),
+               "vs": "FP64 pipeline from the raw traces: FP64 rho filter (ktmApplyRhoFilter.m, "
+                     "3-D i*omega), then FP64 migration (linear pick, |tau| sqrt(t) per pair)",
+               "sample": (f"seeded random {len(xs)}x{len(ys)}x{nz} subgrid of each rank's tile, "
+                          f"batch 0 ({sbounds[0][1] - sbounds[0][0]} survey traces); max over ranks"),
+               "kernel_only": {"rel_l2": allmax(float((got - ref_k).norm() / ref_k.norm())),
+                               "max_rel": allmax(float((got - ref_k).abs().max() / ref_k.abs().max())),
+                               "vs": "FP64 migration of the device-filtered FP32 traces"}}
         image.copy_(image_keep)
 
     # ---- plain FP32 path (psktmCPU.c arithmetic, bit-exact kernel) on part of a batch
-    kp = max(1, bsz // 4) if not a.skip_plain else 64
-    plain_kw = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+    k0p, k1p = bounds[0]
+    kp = max(1, min(k1p - k0p, bsz // 4)) if not a.skip_plain else 64
+    kp = min(kp, raw.shape[0])
+    plain_kw = dict(imageX=gx, imageY=gy, imageZ=sv.imageZ, dt=sv.dt,
                     midX=coords[0][:kp], midY=coords[1][:kp], offX=coords[2][:kp],
                     offY=coords[3][:kp], traces=raw[:kp], velocity=vel1, mode="reference",
                     pick="truncate", stream=stream)
-    small = dict(plain_kw, midX=coords[0][:64], midY=coords[1][:64], offX=coords[2][:64],
-                 offY=coords[3][:64], traces=raw[:64])
-    pimg = torch.empty(sv.shape, device=dev, dtype=torch.float32)
+    ks = min(64, kp)
+    small = dict(plain_kw, midX=coords[0][:ks], midY=coords[1][:ks], offX=coords[2][:ks],
+                 offY=coords[3][:ks], traces=raw[:ks])
+    pimg = torch.empty((tnx, tny, nz), device=dev, dtype=torch.float32)
     ktm.migrate(image=pimg, **small)
     stream.synchronize()
     pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -649,48 +802,50 @@ def main():
     pe1.record(stream)
     stream.synchronize()
     plain_ms = pe0.elapsed_time(pe1)
-    plain_rate = npts * kp / (plain_ms * 1e-3) / 1e9
+    plain_rate = tpts * kp / (plain_ms * 1e-3) / 1e9
     del pimg
 
-    # ---- end to end through the C ABI with host buffers (pinned), per batch:
-    # traces, coordinates, velocity cube host->device, image device->host
+    # ---- end to end through the C ABI with host buffers (pinned), per step: this rank's
+    # traces of batch 0, their coordinates and the tile's Vrms host->device, the tile
+    # image device->host; as many steps as the device-timed measurement
     e2e = None
-    if a.e2e_steps > 0:
+    e2e_steps = a.steps if a.e2e_steps is None else a.e2e_steps
+    if e2e_steps > 0:
         k0, k1 = bounds[0]
         n = k1 - k0
         h_tr = torch.empty((n, sv.nt), dtype=torch.float32, pin_memory=True)
         h_tr.copy_(raw[k0:k1])
         h_c = [torch.empty(n, dtype=torch.float32, pin_memory=True).copy_(c[k0:k1]) for c in coords]
         h_v = torch.empty(vel.shape, dtype=torch.float32, pin_memory=True).copy_(vel)
-        h_img = torch.empty(sv.shape, dtype=torch.float32, pin_memory=True)
-        hk = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
-                  midX=h_c[0].numpy(), midY=h_c[1].numpy(), offX=h_c[2].numpy(),
+        h_img = torch.empty((tnx, tny, nz), dtype=torch.float32, pin_memory=True)
+        hk = dict(midX=h_c[0].numpy(), midY=h_c[1].numpy(), offX=h_c[2].numpy(),
                   offY=h_c[3].numpy(), traces=h_tr.numpy(), velocity=h_v.numpy(),
-                  image=h_img.numpy(), pick="linear", aperture=sv.aperture, rho=sv.rho_opt,
-                  pack_format=a.fmt, weight=a.weight, stream=stream)
+                  image=h_img.numpy(), rho=sv.rho_opt, pack_format=a.fmt, weight=a.weight,
+                  stream=stream, **geo)
         ktm.migrate(**hk)   # warm-up
+        if dist:
+            dist.barrier()
         he0, he1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         he0.record(stream)
-        for _ in range(a.e2e_steps):
+        for _ in range(e2e_steps):
             ktm.migrate(**hk)
         he1.record(stream)
         stream.synchronize()
         wall = time.perf_counter() - t0
-        e_ms = max(he0.elapsed_time(he1), wall * 1e3) / a.e2e_steps
-        if dist:                                   # the slowest rank's time, as for value
-            t = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = allmax(max(he0.elapsed_time(he1), wall * 1e3) / e2e_steps)
         h2d = n * sv.nt * 4 + 4 * n * 4 + vel.numel() * 4
-        e2e = {"value": npts * n / (e_ms * 1e-3) / 1e9 * world, "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 4),
-               "steps": a.e2e_steps, "per_step": "one batch through ktmMigrate, host memory"}
+        e2e = {"value": npts * (sbounds[0][1] - sbounds[0][0]) / (e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(allsum(float(h2d))),
+               "d2h_bytes_per_step": int(allsum(float(tpts * 4))),
+               "steps": e2e_steps,
+               "per_step": "each rank's traces of one batch through ktmMigrate, host memory; "
+                           "max over ranks"}
 
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        sub = synth.config2(ntr=4096, seed=2)
+        sub = synth.config2(ntr=8192, seed=2)
         r, cores, kind, sample = cpu_reference_rate(sub, a.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
         if kind == "reference" and cores > 1:
@@ -699,35 +854,35 @@ def main():
             r1, _, _, s1 = cpu_reference_rate(sub, a.cpu_seconds / 3, 1)
             cpu["one_thread"] = {"value": r1 / 1e9, "sample": s1}
 
-    # DRAM bytes of one step from the ncu capture summarised in profiles/ (one step of
-    # the same workload), scaled to this batch by its traces
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "migrate_fast_traffic.txt")
-    if os.path.exists(tf):
-        kv = dict(line.split(":", 1) for line in open(tf) if ":" in line and not line.startswith("#"))
-        try:
-            traffic = float(kv["dram_bytes_per_step"]) / float(kv["traces_per_step"]) * bsz
-        except (KeyError, ValueError):
-            traffic = None
-
     if rank == 0:
         per_launch_ms = kernel_ms / a.steps
         # binding roofline: the special-function unit.  Fixed algorithmic work per
         # pair: 3 MUFU ops (2 DSR square roots + 1 for the weight sqrt(t)) and 17 FP32
         # flops, so the pair ceiling is min(MUFU peak / 3, FP32 peak / 17); both
-        # peaks measured now on this GPU (ktmProbePeaks)
+        # peaks measured now on this GPU (ktmProbePeaks).  Rank 0's own kernel.
         eval_rate = evaluated / (kernel_ms * 1e-3)
+        if cpu:
+            # psktmCPU.c evaluates every pair; the GPU kernel skips pairs outside the
+            # aperture and past the trace end, so beside the raw ratio: evaluated pairs
+            cpu["gpu_over_cpu"] = {"raw": value / cpu["value"],
+                                   "same_work": eval_rate / 1e9 / cpu["value"],
+                                   "note": "raw: value / this baseline; same_work: the GPU "
+                                           "kernel's evaluated (in-aperture) pairs/s / this "
+                                           "baseline, which evaluates every pair"}
         # our kernels per step: ktmPrepareTraces (1) + the migration, one launch per
         # trace block of at most 40 MB of packed samples (ktm_fast.cu)
         esz = 4 if a.fmt == "f32" else 2
         blk = max(1024, (40 << 20) // (pitch * esz))
-        nblk = -(-bsz // blk)
-        launches = a.steps * (1 + nblk)
+        launches = sum(1 + -(-(bounds[i % nb][1] - bounds[i % nb][0]) // blk)
+                       for i in range(a.steps) if bounds[i % nb][1] > bounds[i % nb][0])
         pair_peak = min(sq.value / 3.0, 2.0 * fm.value / 17.0)
+        rank_b = bounds[0][1] - bounds[0][0]
+        balance = [r["evaluated_pairs"] for r in per_rank]
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": f"{a.fmt} traces, f32 accumulate",
+            "scaling": "strong" if world > 1 else "weak",
+            "vs_baseline": None, "dtype": f"{a.fmt} traces, f32 accumulate",
             "data": "synthetic (seeded, device-generated)",
             "config": {"workload": WORKLOAD, "traces": sv.ntr, "image": [nx, ny, nz],
                        "batch_traces": bsz, "trace_format": a.fmt, "rho": "3D (i*omega)",
@@ -735,28 +890,31 @@ def main():
                        "weight": {"prefold": "sqrt(j dt) folded into the packed samples",
                                   "table": "sqrt(t) from the interpolated sqrt(j dt) table",
                                   "sqrt": "sqrt(t) by sqrt.approx per pair"}[a.weight],
-                       "l2": "each step reads a new 375 MB batch (> 126 MB L2)",
-                       "parallelism": f"{world} GPU(s), one image tile per GPU, no collective"},
+                       "l2": "each step reads a new batch of traces (375 MB raw at N=1, > 126 MB L2)",
+                       "parallelism": (f"output tiles: the {nx}x{ny} image of one survey cut into "
+                                       f"{world} tile(s) (ktm.shard.tile_partition), each rank "
+                                       "migrating the traces its tile's aperture selects "
+                                       "(FP64 host cull); no collective in the data path")},
+            "per_rank": per_rank,
+            "imbalance": (max(balance) / (sum(balance) / len(balance))) if sum(balance) else None,
             "plain_fp32": {"value": plain_rate, "unit": UNIT,
                            "kernel": "bit-exact psktmCPU.c arithmetic (no aperture: every pair)",
-                           "sample": f"{kp} traces x full image, 1-D velocity",
-                           "mixed_over_plain": value / world / plain_rate,
-                           "mixed_over_plain_same_work": (evaluated / (kernel_ms * 1e-3) / 1e9)
-                                                         / plain_rate,
+                           "sample": f"{kp} traces x rank 0's tile, 1-D velocity",
+                           "mixed_over_plain": tpts * traces_done / (ms_rank * 1e-3) / 1e9
+                                               / plain_rate,
+                           "mixed_over_plain_same_work": eval_rate / 1e9 / plain_rate,
                            "same_work_note": "evaluated (in-aperture) pairs/s of the mixed "
                                              "kernel over the plain kernel's pairs/s"},
-            "error": {"rel_l2": rel_l2, "max_rel": max_err, "vs": "FP64 device evaluation",
-                      "sample": f"seeded random {ncols_err[0]}x{ncols_err[1]}x{nz} subgrid, "
-                                f"batch 0 ({bsz} traces)"},
-            "pairs": {"raw_per_step": npts * bsz, "evaluated_fraction": evaluated / max(1, pairs_rank),
-                      "evaluated_rate_gpair_s": evaluated / (kernel_ms * 1e-3) / 1e9,
-                      "in_aperture_fraction": in_aperture / max(1, pairs_rank),
+            "error": err,
+            "pairs": {"raw_per_step": npts * bsz, "evaluated_fraction": evaluated_all / max(1, job_pairs),
+                      "evaluated_rate_gpair_s": eval_rate / 1e9,
+                      "in_aperture_fraction": in_aperture_all / max(1, job_pairs),
                       "note": "evaluated = in aperture and not past the trace end (kernel "
-                              "counter); in_aperture counted separately in FP64"},
+                              "counter, all ranks); in_aperture counted separately in FP64"},
             "roofline": {"bound": "sfu", "achieved": eval_rate / 1e9, "peak": pair_peak / 1e9,
                          "unit": "Gpair/s", "frac": eval_rate / pair_peak,
-                         "traffic": traffic,
-                         "algorithmic_bytes": bsz * pitch * (4 if a.fmt == "f32" else 2) + npts * 4,
+                         "traffic": MIGRATE_DRAM_BYTES_PER_TRACE * rank_b,
+                         "algorithmic_bytes": rank_b * pitch * esz + tpts * 4,
                          "definition": "evaluated pairs/s over the migrate kernel's event time; "
                                        "peak = min(MUFU/3, FP32 flops/17) pairs/s with the "
                                        "MUFU (sqrt.approx) and FFMA throughputs measured now",
@@ -767,9 +925,7 @@ def main():
                                                  "the samples" if a.weight == "prefold" else
                                                  "2 sqrt.approx per pair, plus the weight's "
                                                  "table lookup or third sqrt.approx")},
-                         "traffic_note": "DRAM read+write of one step (5 launches of the "
-                                         "kernel, one per 40 MB trace block) from one ncu "
-                                         "capture, scaled by traces",
+                         "traffic_note": MIGRATE_DRAM_NOTE,
                          "kernel_ms_per_step": per_launch_ms},
             "peaks_measured": {"sqrt_t_s": sq.value / 1e12, "rsqrt_t_s": rs.value / 1e12,
                                "ffma_t_s": fm.value / 1e12},

@@ -110,9 +110,11 @@ enum {
     KTM_FMT_F32 = 0,
     KTM_FMT_F16 = 1,        /* IEEE half, multiplied by a per-trace FP32 scale */
     KTM_FMT_BF16 = 2,       /* bfloat16, multiplied by a per-trace FP32 scale */
-    KTM_FMT_IBM32 = 3       /* IBM System/360 single precision words (inputData.bin,
+    KTM_FMT_IBM32 = 3,      /* IBM System/360 single precision words (inputData.bin,
                                ioFunctions.c:4-40): raw traces only, converted on the
                                device before filtering and packing */
+    KTM_FMT_F64 = 4         /* double: raw traces of ktmMigrateColumnsF64 only (an FP64
+                               pipeline's reference image); rejected elsewhere */
 };
 
 /* Sample pick. */

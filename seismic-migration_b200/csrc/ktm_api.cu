@@ -241,10 +241,13 @@ int check_waits(cudaStream_t s, bool deviceSync)
     return set_ok();
 }
 
-int check_job(const ktm_job* j)
+// allowF64: KTM_FMT_F64 traces (the FP64 device evaluation only)
+int check_job(const ktm_job* j, bool allowF64 = false)
 {
     if (!j) return set_error(KTM_ERR_ARG, "NULL job");
-    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_IBM32)
+    if (j->traceFormat == KTM_FMT_F64 && !allowF64)
+        return set_error(KTM_ERR_ARG, "KTM_FMT_F64 traces are taken by ktmMigrateColumnsF64 only");
+    if (j->traceFormat < KTM_FMT_F32 || j->traceFormat > KTM_FMT_F64)
         return set_error(KTM_ERR_ARG, "bad traceFormat %d", j->traceFormat);
     if (j->traceFormat == KTM_FMT_IBM32 && (j->traceScale || j->tracesPacked))
         return set_error(KTM_ERR_ARG, "IBM-32 traces are raw: no traceScale, not packed");
@@ -464,10 +467,13 @@ void initTwoAxes(imageGrid* imageY, imageGrid* imageZ, float* imageYY, float* im
 
 int ktmMigrateColumnsF64(const ktm_job* job, const int* columns, int ncols, double* out)
 {
-    int rc = ktm::check_job(job);
+    int rc = ktm::check_job(job, true);
     if (rc) return rc;
     if (!job->deviceMemory)
         return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64 takes device memory");
+    if (job->traceFormat == KTM_FMT_F64 && (job->tracesPacked || job->traceScale))
+        return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64: F64 traces are raw (not packed, "
+                                           "no traceScale)");
     if (ncols < 0 || (!out && ncols > 0)) return ktm::set_error(KTM_ERR_ARG, "bad column list");
     if (job->traceFormat == KTM_FMT_IBM32)
         return ktm::set_error(KTM_ERR_ARG, "ktmMigrateColumnsF64: convert IBM-32 traces first "

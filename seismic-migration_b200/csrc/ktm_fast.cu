@@ -551,6 +551,7 @@ int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double load_any(const void* p, int fmt, size_t idx)
 {
+    if (fmt == KTM_FMT_F64) return static_cast<const double*>(p)[idx];
     if (fmt == KTM_FMT_F32) return (double)static_cast<const float*>(p)[idx];
     if (fmt == KTM_FMT_F16) return (double)__half2float(static_cast<const __half*>(p)[idx]);
     return (double)__bfloat162float(static_cast<const __nv_bfloat16*>(p)[idx]);

@@ -23,7 +23,7 @@ KTM_ERR_TIMEOUT = 6
 KTM_ERR_NODEVICE = 7
 
 KTM_MODE_REFERENCE, KTM_MODE_FAST, KTM_MODE_F64 = 0, 1, 2
-KTM_FMT_F32, KTM_FMT_F16, KTM_FMT_BF16, KTM_FMT_IBM32 = 0, 1, 2, 3
+KTM_FMT_F32, KTM_FMT_F16, KTM_FMT_BF16, KTM_FMT_IBM32, KTM_FMT_F64 = 0, 1, 2, 3, 4
 KTM_PICK_TRUNCATE, KTM_PICK_LINEAR = 0, 1
 KTM_RHO_NONE, KTM_RHO_2D, KTM_RHO_25D, KTM_RHO_3D = 0, 1, 2, 3
 

@@ -18,7 +18,7 @@ from ._lib import ImageGrid, JobParams, KtmError, KtmJob, check, lib
 _PICK = {"truncate": _lib.KTM_PICK_TRUNCATE, "linear": _lib.KTM_PICK_LINEAR}
 _MODE = {"reference": _lib.KTM_MODE_REFERENCE, "fast": _lib.KTM_MODE_FAST}
 _FMT = {"f32": _lib.KTM_FMT_F32, "f16": _lib.KTM_FMT_F16, "bf16": _lib.KTM_FMT_BF16,
-        "ibm32": _lib.KTM_FMT_IBM32}
+        "ibm32": _lib.KTM_FMT_IBM32, "f64": _lib.KTM_FMT_F64}
 
 
 def grid(n: int, step: float, start: float = 0.0) -> ImageGrid:
@@ -209,7 +209,8 @@ class Job:
             nt = packed.nt if packed is not None else traces.shape[1]
             if fmt is None:
                 fmt = {torch.float32: "f32", torch.float16: "f16", torch.bfloat16: "bf16",
-                       torch.int32: "ibm32", torch.uint32: "ibm32"}[traces.dtype]
+                       torch.int32: "ibm32", torch.uint32: "ibm32",
+                       torch.float64: "f64"}[traces.dtype]
             if image is None:
                 image = torch.empty((nx, ny, nz), device=traces.device, dtype=torch.float32)
             for a in (midX, midY, offX, offY, velocity, image, scale):

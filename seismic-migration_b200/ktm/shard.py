@@ -102,29 +102,45 @@ def select_traces(midX, midY, tile: Tile, gx: ImageGrid, gy: ImageGrid, aperture
     return np.nonzero(dx * dx + dy * dy <= r * r)[0]
 
 
+def take_rows(a, idx):
+    """Rows ``idx`` of a numpy array, a torch tensor (gathered on its device) or a
+    packed trace set (samples and per-trace scales)."""
+    from .api import PackedTraces
+    if isinstance(a, PackedTraces):
+        return PackedTraces(take_rows(a.data, idx), take_rows(a.scale, idx), a.nt, a.fmt,
+                            a.prefolded, a.rho)
+    if hasattr(a, "index_select"):
+        import torch
+        return a.index_select(0, torch.as_tensor(np.asarray(idx, np.int64), device=a.device))
+    return a[idx]
+
+
+def tile_velocity(velocity, tile: Tile):
+    """A 1-D velocity as is; a [Nx, Ny, Nz] cube cut to the tile (contiguous)."""
+    if len(getattr(velocity, "shape", ())) != 3:
+        return velocity
+    v = velocity[tile.ix0:tile.ix1, tile.iy0:tile.iy1]
+    return v.contiguous() if hasattr(v, "contiguous") else np.ascontiguousarray(v)
+
+
 def migrate_tile(tile: Tile, *, imageX, imageY, imageZ, midX, midY, offX, offY, traces,
                  velocity, aperture=0.0, migrate=None, take=None, **kw):
     """Image one tile with the traces that reach it.  ``velocity`` is 1-D or the
     full [Nx, Ny, Nz] cube (cut to the tile).  ``take(array, indices)`` gathers
-    the selected traces (numpy fancy indexing by default; pass a torch version
-    for device tensors).  Returns the tile image [tnx, tny, Nz]."""
+    the selected traces (``take_rows`` by default: numpy arrays, torch tensors on
+    their device, packed trace sets).  Returns the tile image [tnx, tny, Nz]."""
     if migrate is None:
         from .api import migrate as migrate   # noqa: PLW0127
     if take is None:
-        take = lambda a, idx: a[idx]  # noqa: E731
+        take = take_rows
     mx = midX.cpu().numpy() if hasattr(midX, "cpu") else midX
     my = midY.cpu().numpy() if hasattr(midY, "cpu") else midY
     idx = select_traces(mx, my, tile, imageX, imageY, aperture)
     tgx, tgy = tile.grids(imageX, imageY)
-    if len(getattr(velocity, "shape", ())) == 3:
-        velocity = velocity[tile.ix0:tile.ix1, tile.iy0:tile.iy1]
-        if hasattr(velocity, "contiguous"):
-            velocity = velocity.contiguous()
-        else:
-            velocity = np.ascontiguousarray(velocity)
     return migrate(imageX=tgx, imageY=tgy, imageZ=imageZ, midX=take(midX, idx),
                    midY=take(midY, idx), offX=take(offX, idx), offY=take(offY, idx),
-                   traces=take(traces, idx), velocity=velocity, aperture=aperture, **kw)
+                   traces=take(traces, idx), velocity=tile_velocity(velocity, tile),
+                   aperture=aperture, **kw)
 
 
 def gather_tiles(tile_image, tiles: list[Tile], nz: int, group=None, dst: int | None = 0):

@@ -2,7 +2,11 @@
 
 Every job's image from ktmMigrateBatch must match ktmMigrate on the same job
 (the batch adds trace slices with atomics, so sums agree to FP32 rounding), for
-uneven jobs: patch sizes, Nz, trace counts and velocity laws differ per job.
+uneven jobs: patch sizes, Nz, trace counts and velocity laws differ per job;
+and every job of a batch in the benchmark's format (FP16 with a per-trace
+scale, sqrt(j dt) folded in, the rho filter on the device) must be within 1e-3
+relative L2 of the CPU FP64 oracle of the whole pipeline (oracle/rho.py, then
+oracle.migrate_f64 with the reference weight |tau| sqrt(t) per pair).
 """
 from __future__ import annotations
 
@@ -74,3 +78,49 @@ def test_autotune_returns_a_run_and_is_remembered(cuda, ktm_lib):
     img = ktm.migrate(**{**kw, "image": None, "tile_run": r1}).cpu().numpy()
     ref = ktm.migrate(**{**kw, "image": None, "tile_run": 256}).cpu().numpy()
     assert rel_l2(img, ref) < 1e-5
+
+
+def _oracle_pipeline(sv, raw):
+    """FP64 rho filter (ktmApplyRhoFilter.m) and FP64 migration of one job, on the CPU."""
+    import oracle
+    import rho
+    filt = rho.rho_filter_traces(raw, sv.dt * 1e6, sv.rho_opt)
+    return oracle.migrate_f64(sv.imageX, sv.imageY, sv.imageZ, sv.dt, sv.midX, sv.midY, sv.offX,
+                              sv.offY, filt.astype(np.float32), sv.velocity, pick=1,
+                              aperture=sv.aperture)
+
+
+@pytest.mark.parametrize("fmt,gate", [("f16", 1e-3), ("bf16", 4e-3)])
+def test_batch_jobs_against_fp64_oracle(cuda, ktm_lib, fmt, gate):
+    """Per-job error of the batched launch against the FP64 oracle.  FP16 (the
+    batch benchmark's format) is held to the 1e-3 bar on every job.  BF16 keeps 8
+    significant bits (relative rounding error up to 2^-9 per sample), and these
+    patches sum too few coherent traces for it to average out: it measures
+    1.1e-3 to 1.4e-3 on them, so it is held to 4e-3 here; the 1e-3 claim for BF16
+    holds on the full 2-D line (tests/test_full_size_gpu.py)."""
+    import torch
+
+    import ktm
+    from ktm import synth
+    rng = np.random.default_rng(77)
+    jobs, refs = [], []
+    for j in range(5):
+        side = int(rng.integers(4, 14))
+        ntr = int(rng.integers(800, 2500))
+        sv = synth.areal_survey(ntr=ntr, side=side * 25.0 + 1200.0, maxoff=900.0, nx=side,
+                                ny=side, dxy=25.0, nt=350, dt=0.004, nz=int(rng.integers(200, 350)),
+                                nscat=8, freq=25.0, noise=0.05, aperture=600.0, vtop=1500.0,
+                                vbot=2600.0, lateral=0.0, rho_opt=2, seed=300 + j)
+        sv.imageX.imageStart = sv.imageY.imageStart = 600.0
+        raw = synth.synthesize(sv)
+        refs.append(_oracle_pipeline(sv, raw))
+        packed = ktm.prepare(_t(raw, cuda), sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
+        jobs.append(dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+                         midX=_t(sv.midX, cuda), midY=_t(sv.midY, cuda), offX=_t(sv.offX, cuda),
+                         offY=_t(sv.offY, cuda), traces=packed, velocity=_t(sv.velocity, cuda),
+                         pick="linear", aperture=sv.aperture,
+                         image=torch.full(sv.shape, float("nan"), device=cuda)))
+    images = ktm.migrate_batch(jobs)
+    errs = [rel_l2(img.cpu().numpy(), ref) for img, ref in zip(images, refs)]
+    assert all(np.abs(r).max() > 0 for r in refs)
+    assert max(errs) < gate, errs

@@ -36,3 +36,42 @@ def test_reference_arm_other_ranks_exit_quietly():
                           "--steps", "1", "--warmup", "0", "--ref-step-seconds", "0.5"],
                          capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
     assert out.returncode == 0 and not out.stdout.strip()
+
+
+def _bench():
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import bench
+    return bench
+
+
+def test_cpu_sample_fills_every_thread():
+    """The CPU sample is whole waves of the OpenMP team (psktmCPU.c:56 spreads its
+    trace loop over the threads) with at least eight traces per thread."""
+    from ktm import synth
+    bench = _bench()
+    sv = synth.areal_survey(ntr=600, side=1500.0, maxoff=800.0, nx=12, ny=10, dxy=25.0,
+                            nt=300, dt=0.004, nz=300, nscat=3, freq=25.0, noise=0.05,
+                            aperture=1000.0, vtop=1500.0, vbot=2500.0, lateral=0.0, rho_opt=3,
+                            seed=3, name="sizing")
+    for threads in (1, 3, 4):
+        ref = bench.CpuReference(sv, 0.05, threads)
+        assert ref.ntr % ref.threads == 0 and ref.ntr >= 8 * ref.threads
+        assert ref.rate() > 0
+
+
+def test_bench_rho_f64_matches_oracle_restatement():
+    """The bench's FP64 rho filter (torch) against oracle/rho.py (numpy), all three
+    filters, an odd and a power-of-two trace length."""
+    import numpy as np
+    import torch
+
+    import rho
+    bench = _bench()
+    rng = np.random.default_rng(9)
+    for m in (1501, 1024, 7):
+        x = rng.standard_normal((5, m))
+        for opt in (1, 2, 3):
+            got = bench.rho_filter_f64(torch.as_tensor(x), 0.002, opt).numpy()
+            want = rho.rho_filter_traces(x, 0.002 * 1e6, opt)
+            assert np.allclose(got, want, rtol=1e-12, atol=1e-9 * np.abs(want).max()), (m, opt)
