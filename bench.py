@@ -314,9 +314,9 @@ def batch_main(a):
     for f in fmts:
         imgs = [torch.empty(s.shape, device=dev, dtype=torch.float32) for s in surveys]
         jobs = [dict(g, traces=p, image=im) for g, p, im in zip(geos, packs[f], imgs)]
-        tune = ktm.autotune(**jobs[int(np.argmax([s.pairs for s in surveys]))])
+        tune = ktm.autotune_tile(**jobs[int(np.argmax([s.pairs for s in surveys]))])
         for kw in jobs:
-            kw["tile_run"] = tune
+            kw["tile"] = tune
         ktm.migrate_batch(jobs)                               # warm-up
         torch.cuda.synchronize()
         times = []
@@ -329,7 +329,7 @@ def batch_main(a):
             times.append(e0.elapsed_time(e1))
         ms = float(np.median(times))
         runs[f] = {"value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_launch": ms,
-                   "launches": len(times), "tile_run": tune}
+                   "launches": len(times), "tile": tune}
         images[f] = imgs
     # every job's error against the FP64 pipeline from its raw traces, on sampled columns
     per_job = []
@@ -658,6 +658,19 @@ def main():
     geo = dict(imageX=gx, imageY=gy, imageZ=sv.imageZ, dt=sv.dt, pick="linear",
                aperture=sv.aperture)
 
+    # tile shape (tau run x columns per CTA x traces per chunk) from the tuner, timed on
+    # this rank's first batch; --tile-run fixes the run and keeps the default shape
+    if a.tile_run:
+        tile = {"tileRun": a.tile_run, "tileCols": 0, "tileChunk": 0}
+    else:
+        k0, k1 = bounds[0]
+        p0 = ktm.prepare(raw[k0:k1], sv.dt, fmt=a.fmt, rho=sv.rho_opt, prefold=a.weight == "prefold",
+                         out=pbuf[:k1 - k0], out_scale=pscale[:k1 - k0])
+        tile = ktm.autotune_tile(midX=coords[0][k0:k1], midY=coords[1][k0:k1], offX=coords[2][k0:k1],
+                                 offY=coords[3][k0:k1], traces=p0, velocity=vel, image=image,
+                                 weight=a.weight, **geo)
+        image.zero_()
+
     def step(i, count=False):
         k0, k1 = bounds[i % nb]
         n = k1 - k0
@@ -676,7 +689,7 @@ def main():
                         offY=coords[3][k0:k1], traces=p, velocity=vel, image=image,
                         accumulate=(i > 0), stream=stream,
                         pairs_counter=counter if count else None, weight=a.weight,
-                        tile_run=a.tile_run, **geo)
+                        tile=tile, **geo)
             e1.record(stream)
         return e0, e1, n
 
@@ -886,7 +899,7 @@ def main():
             "data": "synthetic (seeded, device-generated)",
             "config": {"workload": WORKLOAD, "traces": sv.ntr, "image": [nx, ny, nz],
                        "batch_traces": bsz, "trace_format": a.fmt, "rho": "3D (i*omega)",
-                       "pick": "linear", "aperture_m": sv.aperture,
+                       "pick": "linear", "aperture_m": sv.aperture, "tile": tile,
                        "weight": {"prefold": "sqrt(j dt) folded into the packed samples",
                                   "table": "sqrt(t) from the interpolated sqrt(j dt) table",
                                   "sqrt": "sqrt(t) by sqrt.approx per pair"}[a.weight],

@@ -150,9 +150,14 @@ typedef struct ktm_job {
     int   deviceMemory;                        /* 1: every pointer is device memory;
                                                   0: host memory, copied in and out */
     void* stream;                              /* cudaStream_t (NULL: legacy default) */
-    int   tileRun;                             /* tau samples per thread (0: tuned) */
-    int   tileCols;                            /* not read: a fast-kernel CTA always covers
-                                                  8 image columns (one per warp); keep 0 */
+    int   tileRun;                             /* FAST mode: tau samples per warp run, 256,
+                                                  384 or 512 (0: the run wasting the fewest
+                                                  samples of Nz) */
+    int   tileCols;                            /* FAST mode: image columns per CTA, one per
+                                                  warp: 24 (one CTA per SM, the default for
+                                                  0), 12 (two) or 8 (three); 12 and 8 serve the
+                                                  linear pick with the prefolded or table
+                                                  weight.  ktmAutotuneTile chooses these. */
     unsigned long long* pairsEvaluated;        /* optional device counter: pairs the
                                                   kernel evaluated (after culling) */
     /* FAST mode with raw (not packed) traces: the library prepares them first */
@@ -161,6 +166,8 @@ typedef struct ktm_job {
     int   weightMethod;                        /* KTM_WEIGHT_*: how FAST mode evaluates the
                                                   sqrt(t) of the weight when the samples
                                                   do not carry it */
+    int   tileChunk;                           /* FAST mode: traces staged per shared-memory
+                                                  chunk at most (0: as many as fit, <= 32) */
 } ktm_job;
 
 /* sqrt(t) of the reference weight t*sqrt(tau^2/t) = |tau| sqrt(t) (psktmCPU.c:85). */
@@ -293,10 +300,33 @@ int ktmLeastSquaresMigrate(const ktm_lsm* lsm);
  * Images are overwritten.  Asynchronous on `stream`. */
 int ktmMigrateBatch(const ktm_job* jobs, int njobs, void* stream);
 
-/* Tile tuning: times the fast kernel's tau-run length (256, 384, 512 samples per
- * warp) on up to 4096 of the job's traces and returns the fastest in *tileRun
- * (remembered per image / trace shape, format, pick and weight for the process).
- * Overwrites job->image.  Device memory, packed traces; synchronous. */
+/* Tile shape of the fast kernel (ktm_job.tileRun / tileCols / tileChunk).  The
+ * reference's GPU kernel fixes its tile at compile time (THREADS_X x THREADS_Y,
+ * psktmCUDA.cu:95-106); here it is chosen per job shape. */
+typedef struct ktm_tile {
+    int   tileRun;       /* tau samples per warp run: 512, 384 or 256 */
+    int   tileCols;      /* image columns per CTA (one per warp): 24, 12 or 8 */
+    int   tileChunk;     /* traces per shared-memory chunk at most (0: as many as fit) */
+    int   ctasPerSm;     /* CTAs of that shape resident per SM: 1, 2 or 3 (24 warps) */
+    float ms;            /* ktmAutotuneTile: one launch's time on the tuning sample */
+} ktm_tile;
+
+/* The candidate tiles of a job: tau runs 512 / 384 / 256 x CTA shapes (24, 12
+ * or 8 columns per CTA where the job's path is built for them -- linear pick with
+ * the prefolded or table weight -- else 24) x chunks (as many traces as fit, or
+ * at most 8).  Writes up to `capacity` of them and their number to *count.
+ * No device work.  No counterpart in the reference. */
+int ktmTileCandidates(const ktm_job* job, ktm_tile* out, int capacity, int* count);
+
+/* Tile tuning: times every candidate of ktmTileCandidates on up to 4096 of the
+ * job's traces (a warm-up and two timed launches each) and returns the fastest in
+ * *best (remembered per image / trace shape, format, pick and weight for the
+ * process).  Overwrites job->image.  Device memory, packed traces; synchronous.
+ * No counterpart in the reference. */
+int ktmAutotuneTile(const ktm_job* job, ktm_tile* best);
+
+/* ktmAutotuneTile, returning only the chosen tau run (the whole tile is
+ * remembered the same way). */
 int ktmAutotune(const ktm_job* job, int* tileRun);
 
 /* ktmMigrate for callers that cannot allocate device memory while they run:

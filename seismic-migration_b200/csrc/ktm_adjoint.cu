@@ -156,15 +156,30 @@ demigrate_merge_kernel(AdjArgs a)
                 smin = fminf(smin, __shfl_xor_sync(0xffffffffu, smin, o));
             }
             if (!__any_sync(0xffffffffu, any)) continue;        // zero model in this run
-            for (int c = 0; c < n; c++) {
-                const float mx = crd[c], my = crd[a.chunk + c], ox = crd[2 * a.chunk + c],
-                            oy = crd[3 * a.chunk + c];
+            // lane c evaluates trace c's geometry for this column and run (chunk <= 32):
+            // squared source / receiver distances and the keep flag (aperture, and a
+            // lower bound of u over the run below the trace end); the warp then walks
+            // the kept traces in increasing c, taking their distances by shuffle
+            float lds_ = 0.0f, ldr_ = 0.0f;
+            bool keep = false;
+            if (lane < n) {
+                const float mx = crd[lane], my = crd[a.chunk + lane], ox = crd[2 * a.chunk + lane],
+                            oy = crd[3 * a.chunk + lane];
                 const float dmx = mx - cx, dmy = my - cy;
-                if (ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2) continue;
+                keep = !(ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2);
                 const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
-                const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
-                const float ulb = sqrt_approx(fmaf(ds, smin, t2min)) + sqrt_approx(fmaf(dr, smin, t2min));
-                if (!(ulb < umax * 1.0001f + 1.0f)) continue;   // past the trace end (warp-uniform)
+                lds_ = sx * sx + sy * sy;
+                ldr_ = rx * rx + ry * ry;
+                if (keep) {
+                    const float ulb = sqrt_approx(fmaf(lds_, smin, t2min)) +
+                                      sqrt_approx(fmaf(ldr_, smin, t2min));
+                    keep = ulb < umax * 1.0001f + 1.0f;          // not past the trace end
+                }
+            }
+            for (unsigned kept = __ballot_sync(0xffffffffu, keep); kept; kept &= kept - 1u) {
+                const int c = __ffs(kept) - 1;
+                const float ds = __shfl_sync(0xffffffffu, lds_, c);
+                const float dr = __shfl_sync(0xffffffffu, ldr_, c);
                 const unsigned rowS = accS + (unsigned)(c * a.pitch) * 4u;
                 const f2 DS = pk(ds, ds), DR = pk(dr, dr);
                 unsigned qc = 0u;

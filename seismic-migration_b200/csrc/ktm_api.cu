@@ -163,7 +163,7 @@ int run_device(const ktm_job* j, const Geometry& g, const float* midX, const flo
         a.vel = vel; a.velCube = j->velocityCube;
         a.image = image; a.accumulate = j->accumulate;
         a.pick = j->pick; a.aperture = j->aperture;
-        a.tileRun = j->tileRun; a.tileCols = j->tileCols;
+        a.tileRun = j->tileRun; a.tileCols = j->tileCols; a.chunkCap = j->tileChunk;
         a.pairsEvaluated = j->pairsEvaluated;
         // weight sqrt(t): from the kernel's table / sqrt (0) or folded into the packed samples (2)
         a.weightMode = (j->tracesPacked && j->tracesPrefolded) ? 2 : 0;
@@ -579,6 +579,8 @@ int packed_args(const ktm_job* j, FastArgs* a)
     a->image = j->image; a->accumulate = j->accumulate;
     a->pick = j->pick; a->aperture = j->aperture;
     a->tileRun = j->tileRun;
+    a->tileCols = j->tileCols;
+    a->chunkCap = j->tileChunk;
     a->pairsEvaluated = j->pairsEvaluated;
     return KTM_OK;
 }
@@ -593,7 +595,101 @@ struct TuneKey {
     }
 };
 std::mutex g_tuneMu;
-std::map<TuneKey, int> g_tuned;
+std::map<TuneKey, ktm_tile> g_tuned;
+
+// The fast kernel's CTA shapes: columns per CTA and CTAs resident per SM (ktm_fast.cu).
+int ctas_per_sm(int cols) { return cols == 8 ? 3 : cols == 12 ? 2 : 1; }
+
+// Candidate tiles of a job: tau runs 512 / 384 / 256 x CTA shapes (24 x 1, 12 x 2,
+// 8 x 3 columns x CTAs per SM where the path is built for them, else 24 x 1) x
+// traces per chunk (as many as fit, or at most 8).
+std::vector<ktm_tile> tile_candidates(const FastArgs& a)
+{
+    const bool tunable = a.pick == KTM_PICK_LINEAR &&
+                         (a.weightMode == 2 || a.weightMethod == KTM_WEIGHT_TABLE);
+    std::vector<ktm_tile> out;
+    for (int run : {512, 384, 256})
+        for (int cols : {24, 12, 8}) {
+            if (!tunable && cols != 24) continue;
+            for (int chunk : {0, 8}) {
+                ktm_tile t;
+                std::memset(&t, 0, sizeof(t));
+                t.tileRun = run; t.tileCols = cols; t.tileChunk = chunk;
+                t.ctasPerSm = ctas_per_sm(cols);
+                out.push_back(t);
+            }
+        }
+    return out;
+}
+
+TuneKey tune_key(const FastArgs& a)
+{
+    TuneKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.nx = a.g.nx; key.ny = a.g.ny; key.nz = a.g.nz; key.nt = a.g.nt; key.fmt = a.fmt;
+    key.pick = a.pick; key.weightMode = a.weightMode; key.weightMethod = a.weightMethod;
+    return key;
+}
+
+// Times every candidate on up to kTuneTraces of the job's traces (one warm-up and
+// two timed launches each, CUDA events on the job's stream) and returns the fastest.
+constexpr int kTuneTraces = 4096;
+int autotune_tile(const ktm_job* job, ktm_tile* best)
+{
+    FastArgs a;
+    int rc = packed_args(job, &a);
+    if (rc) return rc;
+    const TuneKey key = tune_key(a);
+    {
+        std::lock_guard<std::mutex> lock(g_tuneMu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            *best = it->second;
+            return KTM_OK;
+        }
+    }
+    if ((long long)a.g.nx * a.g.ny * a.g.nz == 0 || a.g.ntr == 0) {
+        // nothing to time: the default shape
+        std::memset(best, 0, sizeof(*best));
+        best->tileRun = 32 * 16; best->tileCols = 24; best->ctasPerSm = 1;
+        return KTM_OK;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(job->stream);
+    a.g.ntr = std::min(a.g.ntr, kTuneTraces);
+    a.accumulate = 0;
+    a.pairsEvaluated = nullptr;
+    cudaEvent_t e0, e1;
+    KTM_CUDA_TRY(cudaEventCreate(&e0));
+    KTM_CUDA_TRY(cudaEventCreate(&e1));
+    ktm_tile chosen;
+    std::memset(&chosen, 0, sizeof(chosen));
+    float bestMs = 3.0e38f;
+    for (ktm_tile t : tile_candidates(a)) {
+        a.tileRun = t.tileRun; a.tileCols = t.tileCols; a.chunkCap = t.tileChunk;
+        if ((rc = launch_fast(a, s))) break;               // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 2 && !rc; r++) rc = launch_fast(a, s);
+        cudaEventRecord(e1, s);
+        if (rc) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = set_error(KTM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t.ms = ms / 2.0f;
+        if (t.ms < bestMs) { bestMs = t.ms; chosen = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lock(g_tuneMu);
+        g_tuned[key] = chosen;
+    }
+    *best = chosen;
+    return KTM_OK;
+}
 
 }  // namespace
 }  // namespace ktm
@@ -613,57 +709,34 @@ extern "C" int ktmMigrateBatch(const ktm_job* jobs, int njobs, void* stream)
     return rc ? rc : set_ok();
 }
 
+extern "C" int ktmAutotuneTile(const ktm_job* job, ktm_tile* best)
+{
+    using namespace ktm;
+    if (!best) return set_error(KTM_ERR_ARG, "NULL tile");
+    const int rc = autotune_tile(job, best);
+    return rc ? rc : set_ok();
+}
+
 extern "C" int ktmAutotune(const ktm_job* job, int* tileRun)
 {
     using namespace ktm;
     if (!tileRun) return set_error(KTM_ERR_ARG, "NULL tileRun");
+    ktm_tile t;
+    const int rc = autotune_tile(job, &t);
+    if (rc) return rc;
+    *tileRun = t.tileRun;
+    return set_ok();
+}
+
+extern "C" int ktmTileCandidates(const ktm_job* job, ktm_tile* out, int capacity, int* count)
+{
+    using namespace ktm;
+    if (!count || capacity < 0 || (capacity > 0 && !out)) return set_error(KTM_ERR_ARG, "bad output");
     FastArgs a;
-    int rc = packed_args(job, &a);
+    const int rc = packed_args(job, &a);
     if (rc) return rc;
-    TuneKey key;
-    std::memset(&key, 0, sizeof(key));
-    key.nx = a.g.nx; key.ny = a.g.ny; key.nz = a.g.nz; key.nt = a.g.nt; key.fmt = a.fmt;
-    key.pick = a.pick; key.weightMode = a.weightMode; key.weightMethod = a.weightMethod;
-    {
-        std::lock_guard<std::mutex> lock(g_tuneMu);
-        auto it = g_tuned.find(key);
-        if (it != g_tuned.end()) {
-            *tileRun = it->second;
-            return set_ok();
-        }
-    }
-    cudaStream_t s = static_cast<cudaStream_t>(job->stream);
-    // time each run length on a sample of the traces (the image is overwritten)
-    a.g.ntr = std::min(a.g.ntr, 4096);
-    a.accumulate = 0;
-    a.pairsEvaluated = nullptr;
-    cudaEvent_t e0, e1;
-    KTM_CUDA_TRY(cudaEventCreate(&e0));
-    KTM_CUDA_TRY(cudaEventCreate(&e1));
-    int best = 0;
-    float bestMs = 3.0e38f;
-    for (int run : {256, 384, 512}) {
-        a.tileRun = run;
-        if ((rc = launch_fast(a, s))) break;               // warm-up
-        cudaEventRecord(e0, s);
-        for (int r = 0; r < 2 && !rc; r++) rc = launch_fast(a, s);
-        cudaEventRecord(e1, s);
-        if (rc) break;
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = set_error(KTM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
-            break;
-        }
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < bestMs) { bestMs = ms; best = run; }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (rc) return rc;
-    {
-        std::lock_guard<std::mutex> lock(g_tuneMu);
-        g_tuned[key] = best;
-    }
-    *tileRun = best;
+    const std::vector<ktm_tile> c = tile_candidates(a);
+    *count = (int)c.size();
+    for (int i = 0; i < (int)c.size() && i < capacity; i++) out[i] = c[i];
     return set_ok();
 }

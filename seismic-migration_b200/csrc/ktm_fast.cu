@@ -22,11 +22,11 @@
 //   u   = min(u, nt)   (also maps NaN to nt, a zero guard)
 //   i0  = floor(u) via the round-down add of 1.5*2^23, f = u - i0
 //   v   = q[i0] + f (q[i0+1] - q[i0]);  acc += s_k * v
-// Work decomposition (148 SMs, three 8-warp CTAs per SM, 80 registers and 74 KB
-// of dynamic shared memory each):
+// Work decomposition (148 SMs, 24 warps per SM at 80 registers; the CTA shape
+// CtaShape below: 24 columns x one CTA per SM by default, 12 x 2 or 8 x 3):
 //   warp   = one image column x a run of 32*R tau samples (lane L owns
 //            tau = run0 + L + 32 r): a warp reads a narrow window of a trace;
-//   CTA    = 8 columns (blockIdx.x) x one run (blockIdx.y) x one slice of the
+//   CTA    = W columns (blockIdx.x) x one run (blockIdx.y) x one slice of the
 //            traces (blockIdx.z); slices write partial images that a second
 //            kernel sums in a fixed order (deterministic), so small images still
 //            fill the GPU;
@@ -37,7 +37,7 @@
 //   cp.async.  For each chunk the CTA first computes per (trace, column) the
 //   squared distances and a skip flag (aperture, or a lower bound of u over the
 //   run beyond the trace end), so the inner loop branches once per trace,
-//   warp-uniformly.
+//   warp-uniformly.  ktmAutotuneTile picks R, the shape and the chunk per job.
 #include "ktm_pair.cuh"
 
 #include <algorithm>
@@ -46,18 +46,36 @@
 namespace ktm {
 namespace {
 
-constexpr int kWarps = 8;
-constexpr int kThreads = kWarps * 32;
-// Three CTAs (24 warps) per SM: 74 KB of dynamic shared memory each (3 x (74 KB +
-// static + 1 KB reserved) fits the SM's 228 KB) and registers capped at 80.  Against
-// two CTAs of 110 KB and 128 registers: 426 instead of 455 ms per 16,384 FP16
-// traces on the 200 x 200 x 1501 image; four CTAs (64 registers) take 478 ms.
-constexpr int kFastMinBlocks = 3;
-constexpr size_t kFastSmemBudget = 74 * 1024;
-// per CTA: the dynamic budget, up to 1 KB of static shared memory (ColInfo,
-// ChunkSync, the batch kernel's FastArgs) and the 1 KB the SM reserves
-static_assert(kFastMinBlocks * (kFastSmemBudget + 2048) <= 228 * 1024,
-              "three CTAs must fit the SM's 228 KB of shared memory");
+// CTA shapes of the fast kernels: warps per CTA (one image column each), CTAs per
+// SM and dynamic shared memory per CTA.  Every shape runs 24 warps per SM with
+// registers capped at 80 (65,536 / 768 threads); MB x (budget + up to 1 KB of
+// static shared memory + the 1 KB the SM reserves) fits the SM's 228 KB.  More
+// columns per CTA share each staged chunk of traces among more warps: on the
+// 200 x 200 x 1501 image, 8192 FP16 traces, 24 x 1 takes 201.8 ms, 12 x 2 203.7
+// ms and 8 x 3 208.6 ms per launch (8 x 2 225.7, 16 x 1 226.8, 4 x 6 229.6).
+// Full = 1: every pick / weight / gradient path is built for the shape; 0: the
+// linear pick with the prefolded or table weight only (the paths the tile
+// tuner searches).
+template <int W, int MB, int KB, int FULL>
+struct CtaShape {
+    static constexpr int kWarps = W;
+    static constexpr int kThreads = W * 32;
+    static constexpr int kMinBlocks = MB;
+    static constexpr size_t kBudget = (size_t)KB * 1024;
+    static constexpr bool kFull = FULL != 0;
+};
+using Shape24 = CtaShape<24, 1, 220, 1>;
+using Shape12 = CtaShape<12, 2, 110, 0>;
+using Shape8 = CtaShape<8, 3, 74, 0>;
+template <class SH>
+constexpr bool shape_fits()
+{
+    return SH::kMinBlocks * (SH::kBudget + 2048) <= 228 * 1024;
+}
+static_assert(shape_fits<Shape24>() && shape_fits<Shape12>() && shape_fits<Shape8>(),
+              "each shape's CTAs must fit the SM's 228 KB of shared memory");
+constexpr int kMaxWarps = 24;
+constexpr int kMaxChunk = 32;
 using namespace dev;
 
 // Bound of one wait for a chunk's bulk copy.  A copy of a chunk takes
@@ -71,7 +89,7 @@ struct ChunkSync {
     unsigned long long bar[2];
     int stalled;
 };
-static_assert(sizeof(ColInfo) * kWarps + sizeof(ChunkSync) + sizeof(FastArgs) + sizeof(int) <= 1024,
+static_assert(sizeof(ColInfo) * kMaxWarps + sizeof(ChunkSync) + sizeof(FastArgs) + sizeof(int) <= 1024,
               "static shared memory of the fast kernels within the 1 KB allowance");
 
 struct ChunkSmem {
@@ -81,6 +99,7 @@ struct ChunkSmem {
 
 // table: the kernel interpolates sqrt(j dt) from a per-CTA table (the table weight);
 // the prefolded and sqrt.approx weights need none, and their chunks grow by its size
+template <int W>
 __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize, int nt,
                                                            bool table)
 {
@@ -88,7 +107,7 @@ __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch,
     L.rawBytes = (size_t)chunk * pitch * esize;              // one buffer
     L.crdOff = 2 * L.rawBytes;                               // [2][5][chunk] floats
     L.geoOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
-    L.wtabOff = L.geoOff + (size_t)chunk * kWarps * sizeof(float4);
+    L.wtabOff = L.geoOff + (size_t)chunk * W * sizeof(float4);
     L.total = L.wtabOff + (table ? (size_t)(nt + 1) * sizeof(float2) : 0);   // [nt+1] weight table
     return L;
 }
@@ -108,10 +127,10 @@ constexpr int kWtTable = 0, kWtPrefold = 1, kWtSqrt = 2;
 // image, or atomic adds into the image (tiles of the batched launch).
 enum { kOutImage = 0, kOutPartial = 1, kOutAtomic = 2 };
 
-// One CTA-tile of the gather: image columns [colGroup*8, colGroup*8+8) x the tau
-// run runIdx x traces [kb, ke).  Used by the grid launch (one tile per CTA) and
-// by the persistent batched launch (a queue of tiles from many jobs).
-template <int R, int PICK, int FMT, int PRE, int GRAD>
+// One CTA-tile of the gather: image columns [colGroup*W, colGroup*W+W) x the tau
+// run runIdx x traces [kb, ke), W = SH::kWarps.  Used by the grid launch (one tile
+// per CTA) and by the persistent batched launch (a queue of tiles from many jobs).
+template <class SH, int R, int PICK, int FMT, int PRE, int GRAD>
 __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colGroup, int runIdx,
                                           int kb, int ke, float* __restrict__ partial, int outMode,
                                           unsigned char* smem_raw, ColInfo* cinfo, ChunkSync& cs)
@@ -119,7 +138,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
     static_assert(R % 2 == 0, "R pairs");
     using T = typename Elem<FMT>::T;
     const Geometry& g = a.g;
-    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt, PRE == kWtTable);
+    const ChunkSmem L = chunk_layout<SH::kWarps>(chunk, a.pitch, sizeof(T), a.g.nt, PRE == kWtTable);
     T* rawBase = reinterpret_cast<T*>(smem_raw);
     float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
     float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
@@ -127,7 +146,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ncols = g.nx * g.ny;
-    const int col = colGroup * kWarps + warp;
+    const int col = colGroup * SH::kWarps + warp;
     const bool colValid = col < ncols;
     const int ci = colValid ? col / g.ny : 0, cj = colValid ? col % g.ny : 0;
     const int run0 = runIdx * (32 * R);
@@ -169,7 +188,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
         cinfo[warp].smin = colValid ? smin : -1.0f;
     }
     if (PRE == kWtTable) {
-        for (int j = threadIdx.x; j <= g.nt; j += kThreads) {
+        for (int j = threadIdx.x; j <= g.nt; j += SH::kThreads) {
             const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
             wtab[j] = make_float2(w0, w1 - w0);
         }
@@ -185,7 +204,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
         const unsigned char* src = static_cast<const unsigned char*>(a.traces) + (size_t)k0 * rowBytes;
         if (threadIdx.x == 0) bulk_g2s(dst, src, (unsigned)((size_t)n * rowBytes), &cs.bar[b]);
         float* crd = crdBase + b * 5 * chunk;
-        for (int q = threadIdx.x; q < 5 * n; q += kThreads) {
+        for (int q = threadIdx.x; q < 5 * n; q += SH::kThreads) {
             const int arr = q / n, c = q % n;
             const float* srcArr = arr == 0 ? a.midX : arr == 1 ? a.midY : arr == 2 ? a.offX
                                 : arr == 3 ? a.offY : a.scale;
@@ -222,8 +241,8 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
         // ---- per (trace, column) distances, scale and skip flag --------------
         {
             const float* crd = crdBase + b * 5 * chunk;
-            for (int p = threadIdx.x; p < chunk * kWarps; p += kThreads) {
-                const int c = p / kWarps, w = p % kWarps;
+            for (int p = threadIdx.x; p < chunk * SH::kWarps; p += SH::kThreads) {
+                const int c = p / SH::kWarps, w = p % SH::kWarps;
                 float4 gd = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
                 const ColInfo cw = cinfo[w];
                 if (c < n && cw.smin >= 0.0f) {
@@ -252,7 +271,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
             const unsigned magicT = (unsigned)kMagicBits * (unsigned)sizeof(T);
             const unsigned wS = smem_u32(wtab) - (unsigned)kMagicBits * 8u;
             for (int c = 0; c < n; c++) {
-                const float4 gd = geo[c * kWarps + warp];
+                const float4 gd = geo[c * SH::kWarps + warp];
                 if (gd.x < 0.0f) continue;                 // warp-uniform
                 keptTraces++;
                 const unsigned rowS = rowsS + (unsigned)(c * a.pitch) * (unsigned)sizeof(T) - magicT;
@@ -369,13 +388,13 @@ struct BatchTile {
     int job, cg, run, kb, ke, pad;
 };
 
-template <int R, int PICK, int FMT, int PRE>
-__global__ void __launch_bounds__(kThreads, kFastMinBlocks)
+template <class SH, int R, int PICK, int FMT, int PRE>
+__global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks)
 batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
              const BatchTile* __restrict__ tiles, int ntiles, unsigned* __restrict__ counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ ColInfo cinfo[kWarps];
+    __shared__ ColInfo cinfo[SH::kWarps];
     __shared__ ChunkSync cs;
     __shared__ FastArgs sa;
     __shared__ int st;
@@ -388,26 +407,26 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
         const BatchTile tl = tiles[t];
         const int* src = reinterpret_cast<const int*>(jobs + tl.job);
         int* dst = reinterpret_cast<int*>(&sa);
-        for (int i = threadIdx.x; i < (int)(sizeof(FastArgs) / 4); i += kThreads) dst[i] = src[i];
+        for (int i = threadIdx.x; i < (int)(sizeof(FastArgs) / 4); i += SH::kThreads) dst[i] = src[i];
         __syncthreads();
-        const bool ok = fast_tile<R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke,
+        const bool ok = fast_tile<SH, R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke,
                                                         nullptr, kOutAtomic, smem_raw, cinfo, cs);
         __syncthreads();                           // shared memory is reused by the next tile
         if (!ok) break;                            // CTA-uniform
     }
 }
 
-template <int R, int PICK, int FMT, int PRE, int GRAD>
-__global__ void __launch_bounds__(kThreads, kFastMinBlocks)
+template <class SH, int R, int PICK, int FMT, int PRE, int GRAD>
+__global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ ColInfo cinfo[kWarps];
+    __shared__ ColInfo cinfo[SH::kWarps];
     __shared__ ChunkSync cs;
     const int kb = blockIdx.z * perSlice;
     const int ke = min(a.g.ntr, kb + perSlice);
     const size_t nimg = (size_t)a.g.nx * a.g.ny * a.g.nz;
-    fast_tile<R, PICK, FMT, PRE, GRAD>(a, chunk, blockIdx.x, blockIdx.y, kb, ke,
+    fast_tile<SH, R, PICK, FMT, PRE, GRAD>(a, chunk, blockIdx.x, blockIdx.y, kb, ke,
                                        partial ? partial + blockIdx.z * nimg : nullptr,
                                        partial ? kOutPartial : kOutImage, smem_raw, cinfo, cs);
 }
@@ -424,28 +443,42 @@ __global__ void reduce_slices(float* __restrict__ out, const float* __restrict__
     }
 }
 
+// Traces per chunk: as many as the shape's shared-memory budget holds (at most
+// kMaxChunk), or fewer when the caller caps them (chunkCap > 0).  0 when even one
+// trace exceeds the largest allocation a CTA can have.
+template <class SH>
+int fast_chunk(const FastArgs& a, int esize, bool table)
+{
+    int chunk = kMaxChunk;
+    if (a.chunkCap > 0) chunk = std::min(chunk, a.chunkCap);
+    while (chunk > 1 && chunk_layout<SH::kWarps>(chunk, a.pitch, esize, a.g.nt, table).total > SH::kBudget)
+        chunk--;
+    if (chunk_layout<SH::kWarps>(chunk, a.pitch, esize, a.g.nt, table).total > (size_t)kMaxSmemBytes)
+        return 0;
+    return chunk;
+}
+
 // One grid launch over all of a's traces.
-template <int R, int PICK, int FMT, int PRE, int GRAD>
+template <class SH, int R, int PICK, int FMT, int PRE, int GRAD>
 int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const Geometry& g = a.g;
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
-    int chunk = 32;
     constexpr bool kTable = PRE == kWtTable;
-    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total > kFastSmemBudget) chunk--;
-    if (chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total > (size_t)kMaxSmemBytes)
+    const int chunk = fast_chunk<SH>(a, esize, kTable);
+    if (chunk == 0)
         return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
                                         "stage limit", a.pitch);
-    const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total;
-    auto kern = fast_kernel<R, PICK, FMT, PRE, GRAD>;
+    const size_t smem = chunk_layout<SH::kWarps>(chunk, a.pitch, esize, g.nt, kTable).total;
+    auto kern = fast_kernel<SH, R, PICK, FMT, PRE, GRAD>;
     KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     const long long cols = (long long)g.nx * g.ny;
-    const unsigned gx = (unsigned)((cols + kWarps - 1) / kWarps);
+    const unsigned gx = (unsigned)((cols + SH::kWarps - 1) / SH::kWarps);
     const unsigned gy = (unsigned)((g.nz + 32 * R - 1) / (32 * R));
     if (gy > 65535) return set_error(KTM_ERR_LIMIT, "fast kernel: Nz too large");
-    // trace slices: about eight CTAs per SM (close to three waves of three resident
-    // CTAs), each slice keeping at least four chunks of traces
+    // trace slices: about eight CTAs per SM over the launch, each slice keeping at
+    // least four chunks of traces
     const long long base = (long long)gx * gy;
     const long long want = 8LL * smCount;
     int slices = (int)((want + base - 1) / base);
@@ -466,7 +499,7 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
         }
     }
     dim3 grid(gx, gy, (unsigned)slices);
-    kern<<<grid, kThreads, smem, stream>>>(a, chunk, perSlice, partial);
+    kern<<<grid, SH::kThreads, smem, stream>>>(a, chunk, perSlice, partial);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && partial) {
         const int th = 256;
@@ -486,13 +519,13 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
 // goes in blocks, one launch each, the later ones accumulating.
 constexpr size_t kTraceBlockBytes = 40u << 20;
 
-template <int R, int PICK, int FMT, int PRE, int GRAD>
+template <class SH, int R, int PICK, int FMT, int PRE, int GRAD>
 int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
 {
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
     const size_t rowBytes = (size_t)a.pitch * esize;
     const int block = (int)std::max<size_t>(1024, kTraceBlockBytes / rowBytes);
-    if (a.g.ntr <= block) return launch_block<R, PICK, FMT, PRE, GRAD>(a, stream, smCount);
+    if (a.g.ntr <= block) return launch_block<SH, R, PICK, FMT, PRE, GRAD>(a, stream, smCount);
     // balanced blocks of at most `block` traces
     const int nblk = (a.g.ntr + block - 1) / block;
     const int per = (a.g.ntr + nblk - 1) / nblk;
@@ -503,45 +536,86 @@ int launch_t(const FastArgs& a, cudaStream_t stream, int smCount)
         b.traces = static_cast<const unsigned char*>(a.traces) + (size_t)kb * rowBytes;
         b.scale = a.scale ? a.scale + kb : nullptr;
         b.accumulate = a.accumulate || kb > 0;
-        const int rc = launch_block<R, PICK, FMT, PRE, GRAD>(b, stream, smCount);
+        const int rc = launch_block<SH, R, PICK, FMT, PRE, GRAD>(b, stream, smCount);
         if (rc) return rc;
     }
     return KTM_OK;
 }
 
-template <int R, int PICK, int PRE, int GRAD = 0>
+template <class SH, int R, int PICK, int PRE, int GRAD = 0>
 int launch_fmt(const FastArgs& a, cudaStream_t s, int sm)
 {
     switch (a.fmt) {
-        case KTM_FMT_F32: return launch_t<R, PICK, KTM_FMT_F32, PRE, GRAD>(a, s, sm);
-        case KTM_FMT_F16: return launch_t<R, PICK, KTM_FMT_F16, PRE, GRAD>(a, s, sm);
-        default: return launch_t<R, PICK, KTM_FMT_BF16, PRE, GRAD>(a, s, sm);
+        case KTM_FMT_F32: return launch_t<SH, R, PICK, KTM_FMT_F32, PRE, GRAD>(a, s, sm);
+        case KTM_FMT_F16: return launch_t<SH, R, PICK, KTM_FMT_F16, PRE, GRAD>(a, s, sm);
+        default: return launch_t<SH, R, PICK, KTM_FMT_BF16, PRE, GRAD>(a, s, sm);
     }
 }
 
-template <int R>
+// The paths a reduced shape is built for: linear pick, prefolded samples or the
+// table weight, no gradient.
+bool tunable_path(const FastArgs& a)
+{
+    return !a.grad && a.pick == KTM_PICK_LINEAR &&
+           (a.weightMode == 2 || a.weightMethod == KTM_WEIGHT_TABLE);
+}
+
+template <class SH, int R>
 int launch_pick(const FastArgs& a, cudaStream_t s, int sm)
 {
-    if (a.grad) {
-        // velocity gradient: linear pick; table weight or prefolded samples
-        if (a.pick != KTM_PICK_LINEAR || (a.weightMode != 2 && a.weightMethod != KTM_WEIGHT_TABLE))
-            return set_error(KTM_ERR_ARG, "ktmVrmsGradient takes the linear pick with the table "
-                                          "weight or prefolded samples");
-        return a.weightMode == 2 ? launch_fmt<R, KTM_PICK_LINEAR, kWtPrefold, 1>(a, s, sm)
-                                 : launch_fmt<R, KTM_PICK_LINEAR, kWtTable, 1>(a, s, sm);
+    if constexpr (!SH::kFull) {
+        if (!tunable_path(a))
+            return set_error(KTM_ERR_ARG, "fast kernel: tileCols %d is built for the linear pick "
+                                          "with the prefolded or table weight only (0 or 24 "
+                                          "takes every path)", SH::kWarps);
+        return a.weightMode == 2 ? launch_fmt<SH, R, KTM_PICK_LINEAR, kWtPrefold>(a, s, sm)
+                                 : launch_fmt<SH, R, KTM_PICK_LINEAR, kWtTable>(a, s, sm);
+    } else {
+        if (a.grad) {
+            // velocity gradient: linear pick; table weight or prefolded samples
+            if (a.pick != KTM_PICK_LINEAR || (a.weightMode != 2 && a.weightMethod != KTM_WEIGHT_TABLE))
+                return set_error(KTM_ERR_ARG, "ktmVrmsGradient takes the linear pick with the table "
+                                              "weight or prefolded samples");
+            return a.weightMode == 2 ? launch_fmt<SH, R, KTM_PICK_LINEAR, kWtPrefold, 1>(a, s, sm)
+                                     : launch_fmt<SH, R, KTM_PICK_LINEAR, kWtTable, 1>(a, s, sm);
+        }
+        // a.weightMode: 2 samples prefolded; otherwise a.weightMethod picks table / sqrt
+        if (a.weightMode == 2) {
+            if (a.pick != KTM_PICK_LINEAR)
+                return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
+            return launch_fmt<SH, R, KTM_PICK_LINEAR, kWtPrefold>(a, s, sm);
+        }
+        const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
+        if (a.pick == KTM_PICK_LINEAR)
+            return sq ? launch_fmt<SH, R, KTM_PICK_LINEAR, kWtSqrt>(a, s, sm)
+                      : launch_fmt<SH, R, KTM_PICK_LINEAR, kWtTable>(a, s, sm);
+        return sq ? launch_fmt<SH, R, KTM_PICK_TRUNCATE, kWtSqrt>(a, s, sm)
+                  : launch_fmt<SH, R, KTM_PICK_TRUNCATE, kWtTable>(a, s, sm);
     }
-    // a.weightMode: 2 samples prefolded; otherwise a.weightMethod picks table / sqrt
-    if (a.weightMode == 2) {
-        if (a.pick != KTM_PICK_LINEAR)
-            return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
-        return launch_fmt<R, KTM_PICK_LINEAR, kWtPrefold>(a, s, sm);
+}
+
+template <class SH>
+int launch_run(const FastArgs& a, int R, cudaStream_t s, int sm)
+{
+    switch (R) {
+        case 8: return launch_pick<SH, 8>(a, s, sm);
+        case 12: return launch_pick<SH, 12>(a, s, sm);
+        case 16: return launch_pick<SH, 16>(a, s, sm);
+        default: return set_error(KTM_ERR_ARG, "fast kernel: tileRun must be 256, 384 or 512");
     }
-    const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
-    if (a.pick == KTM_PICK_LINEAR)
-        return sq ? launch_fmt<R, KTM_PICK_LINEAR, kWtSqrt>(a, s, sm)
-                  : launch_fmt<R, KTM_PICK_LINEAR, kWtTable>(a, s, sm);
-    return sq ? launch_fmt<R, KTM_PICK_TRUNCATE, kWtSqrt>(a, s, sm)
-              : launch_fmt<R, KTM_PICK_TRUNCATE, kWtTable>(a, s, sm);
+}
+
+// tau samples per lane: from tileRun, or the run of 512 / 384 / 256 wasting the
+// fewest samples at the end of Nz
+int choose_run(int tileRun, int nz)
+{
+    if (tileRun > 0) return tileRun / 32;
+    int best = 16, bestWaste = 1 << 30;
+    for (int r : {16, 12, 8}) {
+        const int run = 32 * r, waste = ((nz + run - 1) / run) * run - nz;
+        if (waste < bestWaste) { bestWaste = waste; best = r; }
+    }
+    return best;
 }
 
 // ---------------------------------------------------------------------------
@@ -631,20 +705,13 @@ int launch_fast(const FastArgs& a, cudaStream_t stream)
     int dev = 0, sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
-    int R = a.tileRun > 0 ? a.tileRun / 32 : 0;
-    if (R == 0) {
-        int best = 16, bestWaste = 1 << 30;
-        for (int r : {16, 12, 8}) {
-            const int run = 32 * r, waste = ((g.nz + run - 1) / run) * run - g.nz;
-            if (waste < bestWaste) { bestWaste = waste; best = r; }
-        }
-        R = best;
-    }
-    switch (R) {
-        case 8: return launch_pick<8>(a, stream, sm);
-        case 12: return launch_pick<12>(a, stream, sm);
-        case 16: return launch_pick<16>(a, stream, sm);
-        default: return set_error(KTM_ERR_ARG, "fast kernel: tileRun must be 256, 384 or 512");
+    const int R = choose_run(a.tileRun, g.nz);
+    switch (a.tileCols) {
+        case 0:
+        case 24: return launch_run<Shape24>(a, R, stream, sm);
+        case 12: return launch_run<Shape12>(a, R, stream, sm);
+        case 8: return launch_run<Shape8>(a, R, stream, sm);
+        default: return set_error(KTM_ERR_ARG, "fast kernel: tileCols must be 0, 8, 12 or 24");
     }
 }
 
@@ -663,26 +730,24 @@ int launch_f64_columns(const FastArgs& a, const int* cols, int ncols, double* ou
 namespace ktm {
 namespace {
 
-template <int R, int PICK, int FMT, int PRE>
+template <class SH, int R, int PICK, int FMT, int PRE>
 int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
 {
     const int esize = FMT == KTM_FMT_F32 ? 4 : 2;
     int dev = 0, sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
-    const int ctas = kFastMinBlocks * sm;
+    const int ctas = SH::kMinBlocks * sm;
     std::vector<int> chunks(njobs);
     size_t smem = 0;
     double totalPairs = 0.0;
     for (int j = 0; j < njobs; j++) {
         const Geometry& g = jobs[j].g;
-        int c = 32;
-        while (c > 1 && chunk_layout(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total > kFastSmemBudget)
-            c--;
-        const size_t need = chunk_layout(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total;
-        if (need > (size_t)kMaxSmemBytes)
+        const int c = fast_chunk<SH>(jobs[j], esize, PRE == kWtTable);
+        if (c == 0)
             return set_error(KTM_ERR_LIMIT, "batch: job %d packed pitch %d exceeds shared memory", j,
                              jobs[j].pitch);
+        const size_t need = chunk_layout<SH::kWarps>(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total;
         chunks[j] = c;
         smem = std::max(smem, need);
         totalPairs += (double)g.nx * g.ny * g.nz * g.ntr;
@@ -696,9 +761,9 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
         const Geometry& g = jobs[j].g;
         const long long cols = (long long)g.nx * g.ny;
         if (cols * g.nz == 0 || g.ntr == 0) continue;
-        const int cgs = (int)((cols + kWarps - 1) / kWarps);
+        const int cgs = (int)((cols + SH::kWarps - 1) / SH::kWarps);
         const int runs = (g.nz + 32 * R - 1) / (32 * R);
-        const double tilePairsPerTrace = (double)kWarps * 32 * R;
+        const double tilePairsPerTrace = (double)SH::kWarps * 32 * R;
         int per = (int)std::min<double>(g.ntr, std::max<double>(4.0 * chunks[j], perTile / tilePairsPerTrace));
         per = std::max(per, 1);
         for (int cg = 0; cg < cgs; cg++)
@@ -736,11 +801,11 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
     if (e == cudaSuccess) e = cudaMemcpyAsync(dTiles, sorted.data(), bTiles, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(dCounter, 0, sizeof(unsigned), s);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(batch_kernel<R, PICK, FMT, PRE>,
+        e = cudaFuncSetAttribute(batch_kernel<SH, R, PICK, FMT, PRE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) {
         const int grid = (int)std::min<size_t>((size_t)ctas, sorted.size());
-        batch_kernel<R, PICK, FMT, PRE><<<grid, kThreads, smem, s>>>(dJobs, dChunks, dTiles,
+        batch_kernel<SH, R, PICK, FMT, PRE><<<grid, SH::kThreads, smem, s>>>(dJobs, dChunks, dTiles,
                                                                       (int)sorted.size(), dCounter);
         e = cudaGetLastError();
     }
@@ -750,31 +815,50 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
     return KTM_OK;
 }
 
-template <int R, int PICK, int PRE>
+template <class SH, int R, int PICK, int PRE>
 int launch_batch_fmt(const FastArgs* jobs, int n, cudaStream_t s)
 {
     switch (jobs[0].fmt) {
-        case KTM_FMT_F32: return launch_batch_t<R, PICK, KTM_FMT_F32, PRE>(jobs, n, s);
-        case KTM_FMT_F16: return launch_batch_t<R, PICK, KTM_FMT_F16, PRE>(jobs, n, s);
-        default: return launch_batch_t<R, PICK, KTM_FMT_BF16, PRE>(jobs, n, s);
+        case KTM_FMT_F32: return launch_batch_t<SH, R, PICK, KTM_FMT_F32, PRE>(jobs, n, s);
+        case KTM_FMT_F16: return launch_batch_t<SH, R, PICK, KTM_FMT_F16, PRE>(jobs, n, s);
+        default: return launch_batch_t<SH, R, PICK, KTM_FMT_BF16, PRE>(jobs, n, s);
     }
 }
 
-template <int R>
+template <class SH, int R>
 int launch_batch_r(const FastArgs* jobs, int n, cudaStream_t s)
 {
     const FastArgs& a = jobs[0];
-    if (a.weightMode == 2) {
-        if (a.pick != KTM_PICK_LINEAR)
-            return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
-        return launch_batch_fmt<R, KTM_PICK_LINEAR, kWtPrefold>(jobs, n, s);
+    if constexpr (!SH::kFull) {
+        if (!tunable_path(a))
+            return set_error(KTM_ERR_ARG, "batch: tileCols %d is built for the linear pick with the "
+                                          "prefolded or table weight only", SH::kWarps);
+        return a.weightMode == 2 ? launch_batch_fmt<SH, R, KTM_PICK_LINEAR, kWtPrefold>(jobs, n, s)
+                                 : launch_batch_fmt<SH, R, KTM_PICK_LINEAR, kWtTable>(jobs, n, s);
+    } else {
+        if (a.weightMode == 2) {
+            if (a.pick != KTM_PICK_LINEAR)
+                return set_error(KTM_ERR_ARG, "truncating pick takes traces without the sqrt(t) fold");
+            return launch_batch_fmt<SH, R, KTM_PICK_LINEAR, kWtPrefold>(jobs, n, s);
+        }
+        const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
+        if (a.pick == KTM_PICK_LINEAR)
+            return sq ? launch_batch_fmt<SH, R, KTM_PICK_LINEAR, kWtSqrt>(jobs, n, s)
+                      : launch_batch_fmt<SH, R, KTM_PICK_LINEAR, kWtTable>(jobs, n, s);
+        return sq ? launch_batch_fmt<SH, R, KTM_PICK_TRUNCATE, kWtSqrt>(jobs, n, s)
+                  : launch_batch_fmt<SH, R, KTM_PICK_TRUNCATE, kWtTable>(jobs, n, s);
     }
-    const bool sq = a.weightMethod == KTM_WEIGHT_SQRT;
-    if (a.pick == KTM_PICK_LINEAR)
-        return sq ? launch_batch_fmt<R, KTM_PICK_LINEAR, kWtSqrt>(jobs, n, s)
-                  : launch_batch_fmt<R, KTM_PICK_LINEAR, kWtTable>(jobs, n, s);
-    return sq ? launch_batch_fmt<R, KTM_PICK_TRUNCATE, kWtSqrt>(jobs, n, s)
-              : launch_batch_fmt<R, KTM_PICK_TRUNCATE, kWtTable>(jobs, n, s);
+}
+
+template <class SH>
+int launch_batch_shape(const FastArgs* jobs, int n, int R, cudaStream_t s)
+{
+    switch (R) {
+        case 8: return launch_batch_r<SH, 8>(jobs, n, s);
+        case 12: return launch_batch_r<SH, 12>(jobs, n, s);
+        case 16: return launch_batch_r<SH, 16>(jobs, n, s);
+        default: return set_error(KTM_ERR_ARG, "batch: tileRun must be 256, 384 or 512");
+    }
 }
 
 }  // namespace
@@ -807,11 +891,12 @@ int launch_batch(const FastArgs* jobs, int njobs, cudaStream_t s)
         }
         R = best;
     }
-    switch (R) {
-        case 8: return launch_batch_r<8>(jobs, njobs, s);
-        case 12: return launch_batch_r<12>(jobs, njobs, s);
-        case 16: return launch_batch_r<16>(jobs, njobs, s);
-        default: return set_error(KTM_ERR_ARG, "batch: tileRun must be 256, 384 or 512");
+    switch (a.tileCols) {
+        case 0:
+        case 24: return launch_batch_shape<Shape24>(jobs, njobs, R, s);
+        case 12: return launch_batch_shape<Shape12>(jobs, njobs, R, s);
+        case 8: return launch_batch_shape<Shape8>(jobs, njobs, R, s);
+        default: return set_error(KTM_ERR_ARG, "batch: tileCols must be 0, 8, 12 or 24");
     }
 }
 

@@ -57,7 +57,9 @@ struct FastArgs {
     const float* vel; int velCube;
     float* image; int accumulate;
     int pick; float aperture;
-    int tileRun, tileCols;
+    int tileRun;            // tau samples per warp run (0: chosen from Nz)
+    int tileCols;           // image columns per CTA: 24, 12 or 8 (0: 24)
+    int chunkCap;           // traces per shared-memory chunk at most (0: as many as fit)
     int slices;             // trace slices (0: chosen to fill the GPU)
     int grad;               // 1: write dI/dv (velocity gradient) instead of the image
     void* scratch;          // optional preallocated partial-image buffer

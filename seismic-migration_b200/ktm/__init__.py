@@ -10,5 +10,5 @@ from .api import (  # noqa: F401
     grid, ktmMigrationCPU, ktmMigrationGPU, initThreeAxes, migrate, migrate_columns_f64, Job,
 )
 from .api import PackedTraces, packed_pitch, prepare  # noqa: F401,E402
-from .api import autotune, migrate_batch, interp_time  # noqa: F401,E402
+from .api import autotune, autotune_tile, tile_candidates, migrate_batch, interp_time  # noqa: F401,E402
 from . import io  # noqa: F401,E402

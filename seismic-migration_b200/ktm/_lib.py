@@ -69,7 +69,17 @@ class KtmJob(C.Structure):
         ("tileRun", C.c_int), ("tileCols", C.c_int),
         ("pairsEvaluated", P),
         ("rho", C.c_int), ("packFormat", C.c_int), ("weightMethod", C.c_int),
+        ("tileChunk", C.c_int),
     ]
+
+
+class KtmTile(C.Structure):
+    """ktm_tile (include/ktm.h)."""
+    _fields_ = [("tileRun", C.c_int), ("tileCols", C.c_int), ("tileChunk", C.c_int),
+                ("ctasPerSm", C.c_int), ("ms", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class KtmPrep(C.Structure):
@@ -171,6 +181,11 @@ def lib() -> C.CDLL:
     L.ktmMigrateBatch.restype = C.c_int
     L.ktmAutotune.argtypes = [C.POINTER(KtmJob), C.POINTER(C.c_int)]
     L.ktmAutotune.restype = C.c_int
+    L.ktmAutotuneTile.argtypes = [C.POINTER(KtmJob), C.POINTER(KtmTile)]
+    L.ktmAutotuneTile.restype = C.c_int
+    L.ktmTileCandidates.argtypes = [C.POINTER(KtmJob), C.POINTER(KtmTile), C.c_int,
+                                    C.POINTER(C.c_int)]
+    L.ktmTileCandidates.restype = C.c_int
     L.ktmMigratePackedNoAlloc.argtypes = [C.POINTER(KtmJob)]
     L.ktmMigratePackedNoAlloc.restype = C.c_int
     L.ktmProbePeaks.argtypes = [P, P, P]

@@ -190,7 +190,7 @@ class Job:
                  velocity, image=None, scale=None, mode="fast", pick="linear",
                  aperture=0.0, accumulate=False, prefolded=False, fmt=None, stream=None,
                  tile_run=0, pairs_counter=None, trace_stride=0, rho=0, pack_format="f32",
-                 weight="table"):
+                 weight="table", tile_cols=0, tile_chunk=0, tile=None):
         packed = None
         if isinstance(traces, PackedTraces):
             packed = traces
@@ -252,7 +252,12 @@ class Job:
         j.accumulate = int(bool(accumulate))
         j.deviceMemory = int(dev)
         j.stream = _stream_handle(stream)
+        if tile is not None:                 # a shape from autotune_tile (dict or KtmTile)
+            get = tile.get if isinstance(tile, dict) else lambda k: getattr(tile, k)
+            tile_run, tile_cols, tile_chunk = get("tileRun"), get("tileCols"), get("tileChunk")
         j.tileRun = int(tile_run)
+        j.tileCols = int(tile_cols)
+        j.tileChunk = int(tile_chunk)
         j.pairsEvaluated = _ptr(pairs_counter)
         j.rho = _RHO[rho if not isinstance(rho, str) else rho.lower()]
         j.packFormat = _FMT[pack_format]
@@ -280,11 +285,30 @@ def migrate_batch(jobs, stream=None):
 
 
 def autotune(**kw) -> int:
-    """Fastest tau-run length (tileRun) for this job's shapes (ktmAutotune)."""
+    """The tau run (tileRun) of the fastest tile for this job's shapes (ktmAutotune)."""
     job = Job(**kw)
     out = C.c_int(0)
     check(lib().ktmAutotune(C.byref(job.job), C.byref(out)))
     return int(out.value)
+
+
+def autotune_tile(**kw) -> dict:
+    """The fastest tile shape for this job (ktmAutotuneTile): tileRun, tileCols,
+    tileChunk, ctasPerSm and the measured ms; pass it back as ``tile=``."""
+    job = Job(**kw)
+    t = _lib.KtmTile()
+    check(lib().ktmAutotuneTile(C.byref(job.job), C.byref(t)))
+    return t.as_dict()
+
+
+def tile_candidates(**kw) -> list[dict]:
+    """Every tile shape ktmAutotuneTile times for this job (ktmTileCandidates)."""
+    job = Job(**kw)
+    n = C.c_int(0)
+    check(lib().ktmTileCandidates(C.byref(job.job), None, 0, C.byref(n)))
+    arr = (_lib.KtmTile * max(1, n.value))()
+    check(lib().ktmTileCandidates(C.byref(job.job), arr, n.value, C.byref(n)))
+    return [arr[i].as_dict() for i in range(n.value)]
 
 
 def migrate_columns_f64(*, columns=None, ncols=None, **kw):

@@ -69,15 +69,91 @@ def test_batch_rejects_mixed_formats(cuda, ktm_lib):
         ktm.migrate_batch(a + b)
 
 
-def test_autotune_returns_a_run_and_is_remembered(cuda, ktm_lib):
+def _tune_job(cuda, ntr=3000, side=20, nz=300, nt=350, fmt="f16", seed=90):
+    """One band-limited areal job (2.5-D rho on the device, sqrt(j dt) folded in) and
+    its FP64 oracle image."""
     import ktm
-    kw = make_jobs(cuda, n=1)[0]
-    r1 = ktm.autotune(**kw)
-    assert r1 in (256, 384, 512)
-    assert ktm.autotune(**kw) == r1
-    img = ktm.migrate(**{**kw, "image": None, "tile_run": r1}).cpu().numpy()
-    ref = ktm.migrate(**{**kw, "image": None, "tile_run": 256}).cpu().numpy()
-    assert rel_l2(img, ref) < 1e-5
+    from ktm import synth
+    sv = synth.areal_survey(ntr=ntr, side=side * 25.0 + 1200.0, maxoff=900.0, nx=side, ny=side,
+                            dxy=25.0, nt=nt, dt=0.004, nz=nz, nscat=8, freq=25.0, noise=0.05,
+                            aperture=600.0, vtop=1500.0, vbot=2600.0, lateral=0.0, rho_opt=2,
+                            seed=seed)
+    sv.imageX.imageStart = sv.imageY.imageStart = 600.0
+    raw = synth.synthesize(sv)
+    packed = ktm.prepare(_t(raw, cuda), sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
+    kw = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt,
+              midX=_t(sv.midX, cuda), midY=_t(sv.midY, cuda), offX=_t(sv.offX, cuda),
+              offY=_t(sv.offY, cuda), traces=packed, velocity=_t(sv.velocity, cuda),
+              pick="linear", aperture=sv.aperture, weight="prefold")
+    return sv, raw, kw
+
+
+def test_every_tile_candidate_matches_the_oracle(cuda, ktm_lib):
+    """Every shape the tuner may choose (tau run x columns per CTA x chunk) gives the
+    default shape's image up to FP32 summation order, and the FP64 oracle's to 1e-3."""
+    import ktm
+    sv, raw, kw = _tune_job(cuda)
+    ref = _oracle_pipeline(sv, raw)
+    base = ktm.migrate(**kw).cpu().numpy()
+    cands = ktm.tile_candidates(**kw)
+    assert len(cands) == 18
+    assert {c["tileCols"] for c in cands} == {24, 12, 8}
+    for c in cands:
+        img = ktm.migrate(tile=c, **kw).cpu().numpy()
+        assert np.isfinite(img).all(), c
+        assert rel_l2(img, base) < 1e-5, c
+        assert rel_l2(img, ref) < 1e-3, c
+    # paths built for the default shape only: truncating pick, sqrt weight
+    tkw = dict(kw, traces=ktm.prepare(_t(raw, cuda), sv.dt, fmt="f16", prefold=False),
+               pick="truncate", weight="sqrt")
+    assert {c["tileCols"] for c in ktm.tile_candidates(**tkw)} == {24}
+    with pytest.raises(ktm.KtmError):
+        ktm.migrate(tile_cols=8, **tkw)
+
+
+def test_autotune_tile_is_within_5_percent_of_the_best(cuda, ktm_lib):
+    """The tuner's choice against an exhaustive re-timing of all its candidates on the
+    same job (median of five launches each); remembered per job shape."""
+    import torch
+
+    import ktm
+    _, _, kw = _tune_job(cuda, ntr=4096, side=48, nz=751, nt=751, seed=91)
+    kw["image"] = torch.empty((48, 48, 751), device=cuda)
+    best = ktm.autotune_tile(**kw)
+    assert best["tileRun"] in (256, 384, 512) and best["tileCols"] in (24, 12, 8)
+    assert best["ms"] > 0
+    assert ktm.autotune_tile(**kw) == best
+
+    def timed(tile, reps=5):
+        for _ in range(2):
+            ktm.migrate(tile=tile, **kw)
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ktm.migrate(tile=tile, **kw)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    sweep = {tuple(sorted(c.items())): timed(c) for c in ktm.tile_candidates(**kw)}
+    fastest = min(sweep.values())
+    assert timed(best, reps=9) <= 1.05 * fastest, (best, fastest)
+
+
+def test_batch_takes_a_tuned_tile(cuda, ktm_lib):
+    """The batched launch runs the tuned shape; images equal the default shape's."""
+    import ktm
+    jobs = make_jobs(cuda, fmt="f16", prefold=True)
+    for kw in jobs:
+        kw["weight"] = "prefold"
+    base = [img.clone() for img in ktm.migrate_batch(jobs)]
+    for cols in (12, 8):
+        for kw in jobs:
+            kw["tile"] = {"tileRun": 384, "tileCols": cols, "tileChunk": 0}
+        for img, b in zip(ktm.migrate_batch(jobs), base):
+            assert rel_l2(img.cpu().numpy(), b.cpu().numpy()) < 1e-5
 
 
 def _oracle_pipeline(sv, raw):
