@@ -21,6 +21,7 @@
 
 #include <stddef.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -405,6 +406,36 @@ void ktmFreeSurvey(ktm_survey* s);
 int ktmReadVelModel(const char* path, const ktm_inp* inp, float** velocity, int* velocityCube);
 /* outputData.bin: float32 [Nx][Ny][Nz], tau fastest (ktmVisualizeOutputFile.m:16-28). */
 int ktmWriteImage(const char* path, const float* image, size_t count);
+
+/* The reference's file functions, same names, arguments and behaviour
+ * (ioFunctions.c:44-153), for a caller written against ioFunctions.c.  The
+ * reference uses struct fileInputPtrs without defining it (:96-148 name the
+ * fields); the field order is this library's.  Each records its status for
+ * ktmGetLastError(); ktmLoadSurvey is the checked replacement. */
+struct fileInputPtrs {
+    int   flag;            /* 1 when an input file could not be opened */
+    FILE* inputData;
+    FILE* inputSrcX;
+    FILE* inputSrcY;
+    FILE* inputRecX;
+    FILE* inputRecY;
+};
+/* ioFunctions.c:44-56: whole 4-byte words from the current position to the end;
+ * the file is left at its start. */
+int fileSizeFourBytes(FILE* fin);
+/* ioFunctions.c:60-76: n words from the current position into a new malloc'd
+ * buffer (free it); the file is left at its start.  Words past the end of the
+ * file read as zero here (uninitialised in the reference). */
+unsigned int* binReadUints(FILE* fin, int n);
+float* binReadFloats(FILE* fin, int n);
+/* ioFunctions.c:79-83: t floats to fout. */
+void fileWrite(FILE* fout, float* ptr, int t);
+/* ioFunctions.c:87-90: prints "Can't open <str>." */
+void errorMessage(char* str);
+/* ioFunctions.c:94-153: opens ../data/inputData.bin, inputSrcX.bin, inputSrcY.bin,
+ * inputRecX.bin and inputRecY.bin (relative to the working directory, mode "r+b");
+ * flag = 1 and a message on stdout for each that cannot be opened. */
+void loadInputData(struct fileInputPtrs* input);
 
 /* ioFunctions.c:4-40 (same name and arguments): IBM-32 words to IEEE float,
  * sign * (fraction / 0xFFFFFF) * 16^(exponent - 64), on the current device

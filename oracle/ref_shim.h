@@ -16,12 +16,5 @@
 #define EXPONENT_MASK 0x7f000000u
 #define FRACTION_MASK 0x00ffffffu
 
-/* ioFunctions.c:96-148 uses these fields. */
-struct fileInputPtrs {
-    int flag;
-    FILE* inputData;
-    FILE* inputSrcX;
-    FILE* inputSrcY;
-    FILE* inputRecX;
-    FILE* inputRecY;
-};
+/* struct fileInputPtrs (ioFunctions.c:96-148) comes from ktm.h, so that the
+ * reference's loadInputData and the library's fill the same layout. */

@@ -30,18 +30,20 @@ namespace {
 
 using namespace dev;
 
-constexpr int kAdjWarps = 8;
+// One CTA of 24 warps per SM: the chunk's accumulators get 220 KB (up to 32
+// traces, the lane-parallel geometry's limit) and the registers are capped at 80
+// a thread.  The scatter is latency-bound (shared atomics, square roots).  On the
+// 512 x 1001 line of 32,768 traces, prefolded / table weight: 21.7 / 26.0 ms;
+// 12 warps x two CTAs 22.9 / 27.2; 8 x three (72 KB) 23.6 / 27.7; 16 x one (128
+// registers) 28.2 / 30.9; before that, two CTAs of 100 KB and 115-136 registers
+// 33.4 ms and four CTAs of 64 registers (spilling) 31.9 ms (table weight).
+constexpr int kAdjWarps = 24;
 constexpr int kAdjThreads = kAdjWarps * 32;
 constexpr int kAdjR = 16;                // tau samples per lane per run
-// Three CTAs (24 warps) per SM: the chunk's accumulators fit 72 KB and the
-// registers are capped at 80 a thread.  The scatter is latency-bound (shared
-// atomics, square roots); against two CTAs of 100 KB and 115-136 registers this
-// is 28.7 instead of 33.4 ms on the 512 x 1001 line of 32,768 traces; four CTAs
-// (64 registers) spill and take 31.9 ms.
-constexpr int kAdjMinBlocks = 3;
-constexpr size_t kAdjSmemBudget = 72 * 1024;
+constexpr int kAdjMinBlocks = 1;
+constexpr size_t kAdjSmemBudget = 220 * 1024;
 static_assert(kAdjMinBlocks * (kAdjSmemBudget + 1024) <= 228 * 1024,
-              "three CTAs must fit the SM's 228 KB of shared memory");
+              "the CTAs must fit the SM's 228 KB of shared memory");
 
 struct AdjArgs {
     Geometry g;
@@ -260,7 +262,7 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
     if (g.ntr == 0 || (long long)g.nx * g.ny * g.nz == 0) return KTM_OK;
     const size_t fixed = (size_t)(g.nt + 1) * sizeof(float2) + 64;
     const size_t perTrace = pitchBytes + 4 * sizeof(float);
-    int chunk = 32;
+    int chunk = 32;                     // at most 32: lane c evaluates trace c's geometry
     while (chunk > 1 && fixed + chunk * perTrace > kAdjSmemBudget) chunk--;
     if (fixed + chunk * perTrace > (size_t)kMaxSmemBytes)
         return set_error(KTM_ERR_LIMIT, "demigrate: tracePts=%d exceeds the shared-memory limit", g.nt);

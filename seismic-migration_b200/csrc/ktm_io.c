@@ -12,10 +12,12 @@
  *   velModel.bin    float32 (ktmWriteVelModel.m:22-23): [Nz], or [Nx][Ny][Nz]
  *   outputData.bin  float32 [Nx][Ny][Nz], tau fastest (ktmVisualizeOutputFile.m:16-28)
  *
- * Replaces loadInputData / binReadFloats / binReadUints / fileWrite
- * (ioFunctions.c:44-153): paths are given (not fixed to ../data), sizes come
- * from inp.txt and are checked against the file sizes, and every failure
- * returns KTM_ERR_IO with a message instead of printing.
+ * ktmLoadSurvey and the readers below replace loadInputData / binReadFloats /
+ * binReadUints / fileWrite (ioFunctions.c:44-153): paths are given (not fixed
+ * to ../data), sizes come from inp.txt and are checked against the file sizes,
+ * and every failure returns KTM_ERR_IO with a message instead of printing.
+ * The reference's own names and arguments are exported too, with its
+ * behaviour, for a caller written against ioFunctions.c (end of this file).
  */
 #include <math.h>
 #include <stdarg.h>
@@ -232,4 +234,112 @@ int ktmWriteImage(const char* path, const float* image, size_t count)
     int bad = fclose(f) != 0 || put != count;
     if (bad) return io_fail(KTM_ERR_IO, "cannot write %s", path);
     return ktm_io_ok();
+}
+
+/* ------------------------------------------------------------------------ */
+/* The reference's file functions under its own names (ioFunctions.c:44-153) */
+/* ------------------------------------------------------------------------ */
+
+/* Whole 4-byte words from the current position to the end of the file
+ * (ioFunctions.c:44-56 counts them by reading word after word; the size comes
+ * from the file position here, with the same result), then back to the start. */
+int fileSizeFourBytes(FILE* fin)
+{
+    if (!fin) return io_fail(KTM_ERR_ARG, "fileSizeFourBytes: NULL file"), -1;
+    long words = -1;
+    const long cur = ftell(fin);
+    if (cur >= 0 && fseek(fin, 0, SEEK_END) == 0) {
+        const long end = ftell(fin);
+        if (end >= cur) words = (end - cur) / 4;
+    }
+    if (words < 0) {                         /* not seekable: count as the reference does */
+        unsigned int w;
+        words = 0;
+        while (fread(&w, sizeof(w), 1, fin) == 1) words++;
+    }
+    fseek(fin, 0, SEEK_SET);
+    ktm_io_ok();
+    return (int)words;
+}
+
+/* n words from the current position into a new malloc'd buffer, then back to
+ * the start (ioFunctions.c:60-67, :69-76).  Where the file holds fewer than n,
+ * the rest of the buffer is zero (the reference leaves it uninitialised) and
+ * the status is KTM_ERR_IO. */
+static void* read_n_words(FILE* fin, int n, const char* who)
+{
+    const size_t count = n > 0 ? (size_t)n : 0;
+    unsigned char* p = (unsigned char*)calloc(count ? count : 1, 4);
+    if (!p) {
+        io_fail(KTM_ERR_NOMEM, "%s: cannot allocate %d words", who, n);
+        return NULL;
+    }
+    if (!fin) {
+        io_fail(KTM_ERR_ARG, "%s: NULL file", who);
+        return p;
+    }
+    const size_t got = count ? fread(p, 4, count, fin) : 0;
+    fseek(fin, 0, SEEK_SET);
+    if (got < count) io_fail(KTM_ERR_IO, "%s: %zu of %d words read", who, got, n);
+    else ktm_io_ok();
+    return p;
+}
+
+unsigned int* binReadUints(FILE* fin, int n)
+{
+    return (unsigned int*)read_n_words(fin, n, "binReadUints");
+}
+
+float* binReadFloats(FILE* fin, int n)
+{
+    return (float*)read_n_words(fin, n, "binReadFloats");
+}
+
+/* t floats to fout (ioFunctions.c:79-83). */
+void fileWrite(FILE* fout, float* ptr, int t)
+{
+    if (!fout || (t > 0 && !ptr)) {
+        io_fail(KTM_ERR_ARG, "fileWrite: NULL file or buffer");
+        return;
+    }
+    if (t > 0 && fwrite(ptr, sizeof(float), (size_t)t, fout) != (size_t)t) {
+        io_fail(KTM_ERR_IO, "fileWrite: short write");
+        return;
+    }
+    ktm_io_ok();
+}
+
+/* ioFunctions.c:87-90 */
+void errorMessage(char* str)
+{
+    printf("Can't open %s.\n", str);
+}
+
+/* ioFunctions.c:94-153: the five input files of ../data (relative to the working
+ * directory), opened "r+b" as the reference opens them; a file that cannot be
+ * opened is reported on stdout (errorMessage) and sets flag = 1, the others are
+ * still opened.  The status is KTM_ERR_IO when flag is set. */
+void loadInputData(struct fileInputPtrs* input)
+{
+    static const char* const names[5] = {"../data/inputData.bin", "../data/inputSrcX.bin",
+                                         "../data/inputSrcY.bin", "../data/inputRecX.bin",
+                                         "../data/inputRecY.bin"};
+    if (!input) {
+        io_fail(KTM_ERR_ARG, "loadInputData: NULL input");
+        return;
+    }
+    FILE** slot[5] = {&input->inputData, &input->inputSrcX, &input->inputSrcY,
+                      &input->inputRecX, &input->inputRecY};
+    input->flag = 0;
+    for (int i = 0; i < 5; i++) {
+        FILE* f = fopen(names[i], "r+b");
+        if (!f) {
+            errorMessage((char*)names[i]);
+            input->flag = 1;
+        } else {
+            *slot[i] = f;
+        }
+    }
+    if (input->flag) io_fail(KTM_ERR_IO, "loadInputData: an input file of ../data cannot be opened");
+    else ktm_io_ok();
 }

@@ -151,3 +151,126 @@ def test_psktm_usage_and_missing_directory(ktm_lib, tmp_path):
     assert r.returncode == 1
     r = subprocess.run([PSKTM, str(tmp_path / "absent")], capture_output=True, text=True)
     assert r.returncode == 2 and "inp.txt" in r.stderr
+
+
+# ---- the reference's file functions under their own names (ioFunctions.c:44-153) ----
+
+def _libs():
+    import ctypes as C
+
+    import oracle
+    from conftest import PKG  # noqa: F401
+    import ktm
+    libc = C.CDLL("libc.so.6")
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    libc.ftell.restype = C.c_long
+    libc.ftell.argtypes = [C.c_void_p]
+    libc.fread.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]
+    libc.fread.restype = C.c_size_t
+    libc.free.argtypes = [C.c_void_p]
+    libs = [ktm.lib()]
+    if oracle.ref_available():
+        libs.append(C.CDLL(oracle.REF_SO))
+    for L in libs:
+        L.fileSizeFourBytes.argtypes = [C.c_void_p]
+        L.fileSizeFourBytes.restype = C.c_int
+        for fn in ("binReadUints", "binReadFloats"):
+            getattr(L, fn).argtypes = [C.c_void_p, C.c_int]
+            getattr(L, fn).restype = C.c_void_p
+        L.fileWrite.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.fileWrite.restype = None
+        L.loadInputData.argtypes = [C.c_void_p]
+        L.loadInputData.restype = None
+    return libc, libs
+
+
+class _FileInputPtrs(__import__("ctypes").Structure):
+    import ctypes as _C
+    _fields_ = [("flag", _C.c_int), ("inputData", _C.c_void_p), ("inputSrcX", _C.c_void_p),
+                ("inputSrcY", _C.c_void_p), ("inputRecX", _C.c_void_p), ("inputRecY", _C.c_void_p)]
+
+
+def test_reference_file_functions_match_ioFunctions(tmp_path):
+    """fileSizeFourBytes / binReadUints / binReadFloats / fileWrite of the library
+    against the reference's own compiled ioFunctions.c: same counts, words and
+    bytes, and the file left at its start."""
+    import ctypes as C
+    libc, libs = _libs()
+    words = np.random.default_rng(3).integers(0, 2**32, 1001, dtype=np.uint64).astype(np.uint32)
+    path = tmp_path / "w.bin"
+    path.write_bytes(words.tobytes() + b"\x01\x02\x03")          # 3 stray bytes at the end
+    results = []
+    for k, L in enumerate(libs):
+        f = libc.fopen(str(path).encode(), b"rb")
+        n = L.fileSizeFourBytes(f)
+        pos = libc.ftell(f)
+        pu = L.binReadUints(f, n)
+        u = np.ctypeslib.as_array(C.cast(pu, C.POINTER(C.c_uint32)), (n,)).copy()
+        pf = L.binReadFloats(f, 10)
+        fl = np.ctypeslib.as_array(C.cast(pf, C.POINTER(C.c_float)), (10,)).copy()
+        pos2 = libc.ftell(f)
+        libc.free(pu)
+        libc.free(pf)
+        libc.fclose(f)
+        out = tmp_path / f"out{k}.bin"
+        g = libc.fopen(str(out).encode(), b"wb")
+        vals = np.linspace(-1.0, 1.0, 77).astype(np.float32)
+        L.fileWrite(g, vals.ctypes.data, 77)
+        libc.fclose(g)
+        results.append((n, pos, u, fl, pos2, out.read_bytes()))
+    n, pos, u, fl, pos2, wrote = results[0]
+    assert n == 1001 and pos == 0 and pos2 == 0
+    assert np.array_equal(u, words)
+    assert np.array_equal(fl.view(np.uint32), words[:10])
+    assert wrote == np.linspace(-1.0, 1.0, 77).astype(np.float32).tobytes()
+    for other in results[1:]:                     # the reference's compiled code
+        assert other[0] == n and other[1] == pos and other[4] == pos2
+        assert np.array_equal(other[2], u) and np.array_equal(other[3].view(np.uint32), fl.view(np.uint32))
+        assert other[5] == wrote
+
+
+def test_reference_load_input_data(tmp_path):
+    """loadInputData opens ../data/*.bin relative to the working directory, as the
+    reference does; a missing file sets flag = 1 and prints the reference's message.
+    Run in a child process so that the working directory and stdout are its own."""
+    import subprocess
+    import sys
+    data = tmp_path / "data"
+    work = tmp_path / "work"
+    data.mkdir()
+    work.mkdir()
+    for i, name in enumerate(("inputData", "inputSrcX", "inputSrcY", "inputRecX", "inputRecY")):
+        (data / f"{name}.bin").write_bytes(np.arange(i, i + 8, dtype=np.float32).tobytes())
+    prog = r'''
+import ctypes as C, sys
+sys.path[:0] = sys.argv[1].split(":")
+import test_io
+libc, libs = test_io._libs()
+for L in libs:
+    s = test_io._FileInputPtrs()
+    L.loadInputData(C.byref(s))
+    firsts = []
+    for fld in ("inputData", "inputSrcX", "inputSrcY", "inputRecX", "inputRecY"):
+        f = getattr(s, fld)
+        v = C.c_float()
+        libc.fread(C.byref(v), 4, 1, f) if f else None
+        firsts.append(v.value if f else None)
+    print("RESULT", s.flag, firsts, flush=True)
+'''
+    here = os.path.dirname(os.path.abspath(__file__))
+    pp = ":".join([here, os.path.join(os.path.dirname(here), "seismic-migration_b200"),
+                   os.path.join(os.path.dirname(here), "oracle")])
+    out = subprocess.run([sys.executable, "-c", prog, pp], cwd=work, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT")]
+    assert res and all(r == "RESULT 0 [0.0, 1.0, 2.0, 3.0, 4.0]" for r in res), out.stdout
+    (data / "inputRecX.bin").unlink()
+    out = subprocess.run([sys.executable, "-c", prog, pp], cwd=work, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res = [ln for ln in out.stdout.splitlines() if ln.startswith("RESULT")]
+    assert res and all(r.startswith("RESULT 1 [0.0, 1.0, 2.0, None, 4.0]") for r in res), out.stdout
+    assert out.stdout.count("Can't open ../data/inputRecX.bin.") == len(res)
