@@ -7,7 +7,12 @@
 * one full 62,500-trace step of config 2 (200 x 200 x 1501 image, 3.75e12
   pairs) through the fast path: linearity in the data and invariance to
   splitting the traces into accumulated parts, to FP32 rounding -- size-
-  independent properties where no oracle finishes in seconds.
+  independent properties where no oracle finishes in seconds;
+* config 3 on that step: the 3-D batch in FP16 and BF16 (per-trace scale, the
+  3-D rho filter on the device, sqrt(j dt) folded in) against an FP64 pipeline
+  from the same raw traces -- the FP64 rho filter (bench.rho_filter_f64,
+  pinned to oracle/rho.py on the CPU) and the FP64 device migration -- on a
+  seeded subgrid of columns, within 1e-3.
 """
 from __future__ import annotations
 
@@ -94,5 +99,37 @@ def test_config3_mixed_precision_whole_image(cuda, ktm_lib, fmt):
     ref = ktm.migrate_columns_f64(ncols=nx * ny, traces=p32, **geo).double()
     p = ktm.prepare(raw, sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
     got = ktm.migrate(traces=p, **geo).reshape(nx * ny, nz).double()
+    err = float((got - ref).norm() / ref.norm())
+    assert err < 1e-3, err
+
+
+@pytest.mark.parametrize("fmt", ["f16", "bf16"])
+def test_config3_on_the_3d_step_within_1e3_of_the_fp64_pipeline(cuda, ktm_lib, fmt):
+    import os
+    import sys
+
+    import torch
+
+    import ktm
+    from ktm import synth
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+    sv = synth.config2(ntr=62_500, seed=2)
+    T = lambda x: torch.as_tensor(np.ascontiguousarray(x)).to(cuda)  # noqa: E731
+    co = [T(x) for x in (sv.midX, sv.midY, sv.offX, sv.offY)]
+    raw = synth.synthesize_device(sv, device=cuda, coords=co)
+    geo = dict(imageX=sv.imageX, imageY=sv.imageY, imageZ=sv.imageZ, dt=sv.dt, midX=co[0],
+               midY=co[1], offX=co[2], offY=co[3], velocity=T(sv.velocity), pick="linear",
+               aperture=sv.aperture)
+    p = ktm.prepare(raw, sv.dt, fmt=fmt, rho=sv.rho_opt, prefold=True)
+    img = ktm.migrate(traces=p, weight="prefold", **geo)
+    nx, ny, nz = sv.shape
+    rng = np.random.default_rng(23)
+    cols = torch.as_tensor(np.sort(rng.choice(nx * ny, size=256, replace=False)).astype(np.int32))
+    f64 = bench.rho_filter_f64(raw, sv.dt, sv.rho_opt)
+    ref = ktm.migrate_columns_f64(columns=cols, traces=f64, **geo).double()
+    got = img.reshape(nx * ny, nz)[cols.to(cuda).long()].double()
     err = float((got - ref).norm() / ref.norm())
     assert err < 1e-3, err
