@@ -30,20 +30,24 @@ namespace {
 
 using namespace dev;
 
-// One CTA of 24 warps per SM: the chunk's accumulators get 220 KB (up to 32
-// traces, the lane-parallel geometry's limit) and the registers are capped at 80
-// a thread.  The scatter is latency-bound (shared atomics, square roots).  On the
-// 512 x 1001 line of 32,768 traces, prefolded / table weight: 21.7 / 26.0 ms;
-// 12 warps x two CTAs 22.9 / 27.2; 8 x three (72 KB) 23.6 / 27.7; 16 x one (128
-// registers) 28.2 / 30.9; before that, two CTAs of 100 KB and 115-136 registers
-// 33.4 ms and four CTAs of 64 registers (spilling) 31.9 ms (table weight).
-constexpr int kAdjWarps = 24;
+// One CTA of 32 warps per SM, 8 tau samples per lane: the scatter is latency-
+// bound (each FP32 shared reduction is a load / compare-and-swap loop), so more
+// warps hide more of it; 8 samples a lane keep the tau tables small enough for
+// 64 registers.  The chunk's accumulators get 220 KB (up to 32 traces, the
+// lane-parallel geometry's limit).  On the 512 x 1001 line of 32,768 traces,
+// prefolded / table weight: 32 x 1, R = 8: 19.9 / 23.6 ms; R = 16 (spilling) 19.6
+// / 25.1; R = 4 23.1 / 26.2; 20 warps x two CTAs (R = 8) 19.8 / 24.5; 16 x 2 20.7 /
+// 24.4; 24 x 2 (spilling) 20.6 / 26.3; 24 x 1, R = 16, 80 registers 21.7 / 26.0;
+// 8 x 3 (72 KB) 23.6 / 27.7; before that two CTAs of 100 KB 33.4 ms and four CTAs
+// of 64 registers 31.9 ms (table weight, R = 16).
+constexpr int kAdjWarps = 32;
 constexpr int kAdjThreads = kAdjWarps * 32;
-constexpr int kAdjR = 16;                // tau samples per lane per run
+constexpr int kAdjR = 8;                 // tau samples per lane per run
 constexpr int kAdjMinBlocks = 1;
 constexpr size_t kAdjSmemBudget = 220 * 1024;
 static_assert(kAdjMinBlocks * (kAdjSmemBudget + 1024) <= 228 * 1024,
               "the CTAs must fit the SM's 228 KB of shared memory");
+static_assert((kAdjR & (kAdjR - 1)) == 0, "the lane rotation takes a power-of-two run");
 
 struct AdjArgs {
     Geometry g;
@@ -72,15 +76,15 @@ __device__ __forceinline__ void red_shared_if(bool on, unsigned addr, float v)
                  ::"r"(addr), "f"(v), "r"((unsigned)on));
 }
 
-// Lane-private merge of the scatter: lane L owns the 16 CONSECUTIVE tau samples run0 + 16 L + i of a run, so for one trace
-// the target sample floor(u) advances monotonically (mostly by 0 or 1) along
-// the lane's samples.  The lane walks them keeping a running (sample, value,
-// value of the next sample) and issues an atomic only when it leaves a sample:
-// one red.shared per pair where u advances by a sample, fewer where it stalls
-// (shallow, far offsets), two only where it jumps.  Lane L visits its samples
-// starting at i = L mod 16 (slot s holds sample (s + L) mod 16), so at each step
-// the 32 lanes sit 17 samples apart and hit distinct banks; the one wrap per lane
-// is an ordinary jump.
+// Lane-private merge of the scatter: lane L owns the R = kAdjR CONSECUTIVE tau
+// samples run0 + R L + i of a run, so for one trace the target sample floor(u)
+// advances monotonically (mostly by 0 or 1) along the lane's samples.  The lane
+// walks them keeping a running (sample, value, value of the next sample) and
+// issues an atomic only when it leaves a sample: one red.shared per pair where u
+// advances by a sample, fewer where it stalls (shallow, far offsets), two only
+// where it jumps.  Lane L visits its samples starting at i = L mod R (slot s holds
+// sample (s + L) mod R), so at each step the 32 lanes sit R + 1 samples apart and
+// spread over the banks; the one wrap per lane is an ordinary jump.
 // WT: 0 sqrt(j dt) table interpolated per pair, 1 sqrt.approx per pair,
 //     2 prefolded (sqrt(j dt) per output sample at the write-out).
 template <int PICK, int WT>

@@ -200,3 +200,39 @@ def test_batch_jobs_against_fp64_oracle(cuda, ktm_lib, fmt, gate):
     errs = [rel_l2(img.cpu().numpy(), ref) for img, ref in zip(images, refs)]
     assert all(np.abs(r).max() > 0 for r in refs)
     assert max(errs) < gate, errs
+
+
+def test_batch_edge_jobs(cuda, ktm_lib):
+    """Jobs with no traces (image overwritten with zeros), a 1 x 1 image, a single trace,
+    and the tuner on a job with nothing to time (the default tile)."""
+    import torch
+
+    import ktm
+    jobs = make_jobs(cuda, n=3, fmt="f16", prefold=True, seed=5)
+    for kw in jobs:
+        kw["weight"] = "prefold"
+    empty = dict(jobs[0])
+    empty["traces"] = ktm.api.PackedTraces(jobs[0]["traces"].data[:0], jobs[0]["traces"].scale[:0],
+                                           jobs[0]["traces"].nt, "f16", True, 0)
+    for k in ("midX", "midY", "offX", "offY"):
+        empty[k] = jobs[0][k][:0]
+    empty["image"] = torch.full(jobs[0]["image"].shape, float("nan"), device=cuda)
+    one = dict(jobs[1])
+    one["imageX"] = ktm.grid(1, one["imageX"].imageStep, one["imageX"].imageStart)
+    one["imageY"] = ktm.grid(1, one["imageY"].imageStep, one["imageY"].imageStart)
+    one["velocity"] = one["velocity"][:1, :1].contiguous()
+    one["image"] = torch.full((1, 1, jobs[1]["imageZ"].imagePnts), float("nan"), device=cuda)
+    single = dict(jobs[2])
+    single["traces"] = ktm.api.PackedTraces(jobs[2]["traces"].data[:1], jobs[2]["traces"].scale[:1],
+                                            jobs[2]["traces"].nt, "f16", True, 0)
+    for k in ("midX", "midY", "offX", "offY"):
+        single[k] = jobs[2][k][:1]
+    single["image"] = torch.full(jobs[2]["image"].shape, float("nan"), device=cuda)
+    imgs = ktm.migrate_batch([empty, one, single])
+    assert torch.count_nonzero(imgs[0]).item() == 0 and torch.isfinite(imgs[0]).all()
+    for kw, img in zip([one, single], imgs[1:]):
+        ref = ktm.migrate(**{**kw, "image": None}).cpu().numpy()
+        assert np.isfinite(img.cpu().numpy()).all()
+        assert rel_l2(img.cpu().numpy(), ref) < 1e-5 or np.abs(ref).max() == 0
+    tile = ktm.autotune_tile(**empty)      # nothing to time: a valid tile, no launch
+    assert tile["tileCols"] in (24, 12, 8) and tile["tileRun"] in (256, 384, 512)
