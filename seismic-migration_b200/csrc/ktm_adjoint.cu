@@ -13,7 +13,7 @@
 // (ktm_pair.cuh), so the two operators are transposes pair by pair.
 //
 // Work decomposition: a CTA owns a chunk of traces, accumulates their samples
-// in shared memory (red.shared.add) while its warps sweep the image columns of
+// in shared memory (padded rows, red.shared.add) while its warps sweep the image columns of
 // its column block, and writes the chunk out once (plain stores when one block
 // covers all columns, red.global.add otherwise).  A warp covers one column x a
 // run of 32*R tau samples at a time; the model samples, the tau tables and the
@@ -30,24 +30,33 @@ namespace {
 
 using namespace dev;
 
-// One CTA of 32 warps per SM, 8 tau samples per lane: the scatter is latency-
-// bound (each FP32 shared reduction is a load / compare-and-swap loop), so more
-// warps hide more of it; 8 samples a lane keep the tau tables small enough for
-// 64 registers.  The chunk's accumulators get 220 KB (up to 32 traces, the
-// lane-parallel geometry's limit).  On the 512 x 1001 line of 32,768 traces,
-// prefolded / table weight: 32 x 1, R = 8: 19.9 / 23.6 ms; R = 16 (spilling) 19.6
-// / 25.1; R = 4 23.1 / 26.2; 20 warps x two CTAs (R = 8) 19.8 / 24.5; 16 x 2 20.7 /
-// 24.4; 24 x 2 (spilling) 20.6 / 26.3; 24 x 1, R = 16, 80 registers 21.7 / 26.0;
-// 8 x 3 (72 KB) 23.6 / 27.7; before that two CTAs of 100 KB 33.4 ms and four CTAs
-// of 64 registers 31.9 ms (table weight, R = 16).
+// One CTA of 32 warps per SM, 8 tau samples per lane: each FP32 shared reduction
+// is a load / compare-and-swap loop, so more warps hide more of its latency; 8
+// samples a lane keep the tau tables small enough for 64 registers.  The chunk's
+// accumulators get 220 KB (up to 32 traces, the lane-parallel geometry's limit).
+// On the 512 x 1001 line of 32,768 traces, prefolded / table weight, padded rows:
+// 32 x 1, R = 8, a padding word per 4 samples 14.8 / 18.6 ms, per 8 samples 14.9 /
+// 18.9; 16 x 2 15.6 / 19.6; 24 x 1, R = 16 (80 registers) 17.3 / 21.9.  Unpadded
+// rows with the lanes' visiting order rotated against bank conflicts: 32 x 1, R = 8
+// 19.9 / 23.6; R = 16 (spilling) 19.6 / 25.1; 20 x 2 19.8 / 24.5; 24 x 1, R = 16
+// 21.7 / 26.0; 8 x 3 (72 KB) 23.6 / 27.7.
 constexpr int kAdjWarps = 32;
 constexpr int kAdjThreads = kAdjWarps * 32;
 constexpr int kAdjR = 8;                 // tau samples per lane per run
 constexpr int kAdjMinBlocks = 1;
+constexpr int kPadShift = 2;             // one padding word per 4 samples
 constexpr size_t kAdjSmemBudget = 220 * 1024;
 static_assert(kAdjMinBlocks * (kAdjSmemBudget + 1024) <= 228 * 1024,
               "the CTAs must fit the SM's 228 KB of shared memory");
-static_assert((kAdjR & (kAdjR - 1)) == 0, "the lane rotation takes a power-of-two run");
+
+// Accumulator rows and the weight table hold sample j at word j + (j >> kPadShift).
+// At one step of the scatter the lanes of a warp sit R = 8 tau samples apart, so
+// their target samples lie about 8 u' apart (u' = d(t/dt)/dtau in samples per tau
+// sample, 1 at zero offset and less with offset): without padding, multiples of 4 or 8
+// words that share a few banks.  The padding word per 4 samples spreads them.  A row
+// of n holds every j <= n + 1; rounded up to 4 words so that the arrays after the rows
+// stay 16-byte aligned.
+__host__ __device__ __forceinline__ int padded_pitch(int n) { return (n + (n >> kPadShift) + 2 + 3) & ~3; }
 
 struct AdjArgs {
     Geometry g;
@@ -77,14 +86,14 @@ __device__ __forceinline__ void red_shared_if(bool on, unsigned addr, float v)
 }
 
 // Lane-private merge of the scatter: lane L owns the R = kAdjR CONSECUTIVE tau
-// samples run0 + R L + i of a run, so for one trace the target sample floor(u)
-// advances monotonically (mostly by 0 or 1) along the lane's samples.  The lane
-// walks them keeping a running (sample, value, value of the next sample) and
+// samples run0 + R L + i of a run and visits them in increasing tau, so for one
+// trace the target sample floor(u) advances monotonically (mostly by 0 or 1).  The
+// lane walks them keeping a running (sample, value, value of the next sample) and
 // issues an atomic only when it leaves a sample: one red.shared per pair where u
-// advances by a sample, fewer where it stalls (shallow, far offsets), two only
-// where it jumps.  Lane L visits its samples starting at i = L mod R (slot s holds
-// sample (s + L) mod R), so at each step the 32 lanes sit R + 1 samples apart and
-// spread over the banks; the one wrap per lane is an ordinary jump.
+// advances by a sample, fewer where it stalls (shallow, far offsets), two only where
+// it jumps by two or more.  (Visiting the samples in a lane-rotated order instead,
+// against bank conflicts on unpadded rows, made every lane jump once per run and
+// cost 25 % more time.)
 // WT: 0 sqrt(j dt) table interpolated per pair, 1 sqrt.approx per pair,
 //     2 prefolded (sqrt(j dt) per output sample at the write-out).
 template <int PICK, int WT>
@@ -93,13 +102,14 @@ demigrate_merge_kernel(AdjArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Geometry& g = a.g;
-    float* acc = reinterpret_cast<float*>(smem_raw);                    // [chunk][pitch]
-    float* crd = acc + (size_t)a.chunk * a.pitch;                       // [4][chunk]
-    float2* wtab = reinterpret_cast<float2*>(crd + 4 * a.chunk + ((4 * a.chunk) & 1));  // [nt+1]
+    const int pitchP = padded_pitch(a.pitch);
+    float* acc = reinterpret_cast<float*>(smem_raw);                    // [chunk][pitchP]
+    float* crd = acc + (size_t)a.chunk * pitchP;                        // [4][chunk]
+    float2* wtab = reinterpret_cast<float2*>(crd + 4 * a.chunk + ((4 * a.chunk) & 1));  // padded [nt+1]
 
     const int k0 = blockIdx.x * a.chunk;
     const int n = min(a.chunk, g.ntr - k0);
-    for (int i = threadIdx.x; i < a.chunk * a.pitch; i += kAdjThreads) acc[i] = 0.0f;
+    for (int i = threadIdx.x; i < a.chunk * pitchP; i += kAdjThreads) acc[i] = 0.0f;
     for (int i = threadIdx.x; i < n; i += kAdjThreads) {
         crd[i] = a.midX[k0 + i];
         crd[a.chunk + i] = a.midY[k0 + i];
@@ -109,7 +119,7 @@ demigrate_merge_kernel(AdjArgs a)
     if (WT == 0) {
         for (int j = threadIdx.x; j <= g.nt; j += kAdjThreads) {
             const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
-            wtab[j] = make_float2(w0, w1 - w0);
+            wtab[j + (j >> kPadShift)] = make_float2(w0, w1 - w0);
         }
     }
     __syncthreads();
@@ -122,8 +132,11 @@ demigrate_merge_kernel(AdjArgs a)
     const float umax = (float)g.nt;
     const float ap2 = a.aperture > 0.0f ? a.aperture * a.aperture : -1.0f;
     const f2 M2 = pk(kMagic, kMagic);
-    const unsigned accS = smem_u32(acc) - (unsigned)kMagicBits * 4u;
-    const unsigned wS = smem_u32(wtab) - (unsigned)kMagicBits * 8u;
+    // bits(fl) = K + i0, K = kMagicBits a multiple of 4: the padded word of sample i0 is
+    // q + (q >> kPadShift) - kPad, kPad = K + (K >> kPadShift); the row bases carry -kPad
+    const unsigned kPad = (unsigned)kMagicBits + ((unsigned)kMagicBits >> kPadShift);
+    const unsigned accS = smem_u32(acc) - kPad * 4u;
+    const unsigned wS = smem_u32(wtab) - kPad * 8u;
     const int nruns = (g.nz + 32 * kAdjR - 1) / (32 * kAdjR);
 
     for (int col = cb0 + warp; col < cb1; col += kAdjWarps) {
@@ -139,7 +152,7 @@ demigrate_merge_kernel(AdjArgs a)
                 float tv[2], sv[2], mv[2];
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
-                    const int l = base + ((2 * h + e + lane) & (kAdjR - 1));
+                    const int l = base + 2 * h + e;
                     const bool ok = l < g.nz;
                     const int lc = ok ? l : g.nz - 1;
                     const float tau = g.z0 + (float)lc * g.dz;
@@ -186,16 +199,17 @@ demigrate_merge_kernel(AdjArgs a)
                 const int c = __ffs(kept) - 1;
                 const float ds = __shfl_sync(0xffffffffu, lds_, c);
                 const float dr = __shfl_sync(0xffffffffu, ldr_, c);
-                const unsigned rowS = accS + (unsigned)(c * a.pitch) * 4u;
+                const unsigned rowS = accS + (unsigned)(c * pitchP) * 4u;
                 const f2 DS = pk(ds, ds), DR = pk(dr, dr);
-                unsigned qc = 0u;
+                unsigned qc = 0u, pc = 0u;
                 float va = 0.0f, vb = 0.0f;
 #pragma unroll
                 for (int h = 0; h < kAdjR / 2; h++) {
                     const PairKin kk = pair_kin(DS, DR, S2[h], T2[h], umax, M2);
+                    const unsigned pp0 = kk.q0 + (kk.q0 >> kPadShift), pp1 = kk.q1 + (kk.q1 >> kPadShift);
                     f2 VAL;
                     if (WT == 0) {
-                        const float2 w0 = lds_f2(wS + kk.q0 * 8u), w1 = lds_f2(wS + kk.q1 * 8u);
+                        const float2 w0 = lds_f2(wS + pp0 * 8u), w1 = lds_f2(wS + pp1 * 8u);
                         VAL = mul2(fma2(kk.F, pk(w0.y, w1.y), pk(w0.x, w1.x)), MT[h]);
                     } else if (WT == 1) {
                         VAL = mul2(mul2(pk(sqrt_approx(kk.u0), sqrt_approx(kk.u1)),
@@ -214,25 +228,33 @@ demigrate_merge_kernel(AdjArgs a)
                         upk(VAL, ca[0], ca[1]);
                         cb[0] = cb[1] = 0.0f;
                     }
-                    const unsigned qs[2] = {rowS + kk.q0 * 4u, rowS + kk.q1 * 4u};
+                    const unsigned qs[2] = {kk.q0, kk.q1}, ps[2] = {pp0, pp1};
 #pragma unroll
                     for (int e = 0; e < 2; e++) {
                         const unsigned q = qs[e];
                         if (h == 0 && e == 0) {
-                            qc = q; va = ca[0]; vb = cb[0];
+                            qc = q; pc = ps[0]; va = ca[0]; vb = cb[0];
                             continue;
                         }
                         const bool same = q == qc;
-                        const bool next = q == qc + 4u;
-                        red_shared_if(!same, qc, va);
-                        if (PICK == KTM_PICK_LINEAR) red_shared_if(!same && !next, qc + 4u, vb);
+                        const bool next = q == qc + 1u;
+                        red_shared_if(!same, rowS + pc * 4u, va);
+                        if (PICK == KTM_PICK_LINEAR) {
+                            // sample qc + 1 is flushed here only where u jumped by two or more
+                            const unsigned qn = qc + 1u;
+                            red_shared_if(!same && !next, rowS + (qn + (qn >> kPadShift)) * 4u, vb);
+                        }
                         va = same ? va + ca[e] : (next ? vb + ca[e] : ca[e]);
                         vb = same ? vb + cb[e] : cb[e];
                         qc = q;
+                        pc = ps[e];
                     }
                 }
-                red_shared(qc, va);
-                if (PICK == KTM_PICK_LINEAR) red_shared(qc + 4u, vb);
+                red_shared(rowS + pc * 4u, va);
+                if (PICK == KTM_PICK_LINEAR) {
+                    const unsigned qn = qc + 1u;
+                    red_shared(rowS + (qn + (qn >> kPadShift)) * 4u, vb);
+                }
             }
         }
     }
@@ -240,7 +262,7 @@ demigrate_merge_kernel(AdjArgs a)
     __syncthreads();
     for (int i = threadIdx.x; i < n * a.pitch; i += kAdjThreads) {
         const int c = i / a.pitch, j = i % a.pitch;
-        float v = (j > 0 && j < g.nt) ? acc[i] : 0.0f;
+        float v = (j > 0 && j < g.nt) ? acc[(size_t)c * pitchP + j + (j >> kPadShift)] : 0.0f;
         if (WT == 2) v *= sqrtf((float)j * g.dt);        // the fold's factor (ktm_prep.cu, ktm_lsm.cu)
         float* dst = a.data + (size_t)(k0 + c) * a.pitch + j;
         if (a.atomicOut) {
@@ -264,8 +286,8 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
     if (!accumulate && g.ntr > 0)
         KTM_CUDA_TRY(cudaMemsetAsync(data, 0, pitchBytes * g.ntr, s));
     if (g.ntr == 0 || (long long)g.nx * g.ny * g.nz == 0) return KTM_OK;
-    const size_t fixed = (size_t)(g.nt + 1) * sizeof(float2) + 64;
-    const size_t perTrace = pitchBytes + 4 * sizeof(float);
+    const size_t fixed = (size_t)padded_pitch(g.nt + 1) * sizeof(float2) + 64;
+    const size_t perTrace = (size_t)padded_pitch(pitch) * sizeof(float) + 4 * sizeof(float);
     int chunk = 32;                     // at most 32: lane c evaluates trace c's geometry
     while (chunk > 1 && fixed + chunk * perTrace > kAdjSmemBudget) chunk--;
     if (fixed + chunk * perTrace > (size_t)kMaxSmemBytes)

@@ -34,10 +34,11 @@
 //   moves a chunk's packed rows (one contiguous, 16-byte aligned range) with a
 //   single bulk copy (cp.async.bulk) completed on the buffer's mbarrier, waited
 //   for with a one-second bound; the coordinates and scales follow in 4-byte
-//   cp.async.  For each chunk the CTA first computes per (trace, column) the
-//   squared distances and a skip flag (aperture, or a lower bound of u over the
-//   run beyond the trace end), so the inner loop branches once per trace,
-//   warp-uniformly.  ktmAutotuneTile picks R, the shape and the chunk per job.
+//   cp.async.  For each chunk, lane c of every warp computes trace c's squared
+//   distances and skip flag (aperture, or a lower bound of u over the run beyond
+//   the trace end) for the warp's column; the warp walks the kept traces of its
+//   ballot, taking their distances by shuffle, with no second barrier per chunk.
+//   ktmAutotuneTile picks R, the shape and the chunk per job.
 #include "ktm_pair.cuh"
 
 #include <algorithm>
@@ -74,8 +75,7 @@ constexpr bool shape_fits()
 }
 static_assert(shape_fits<Shape24>() && shape_fits<Shape12>() && shape_fits<Shape8>(),
               "each shape's CTAs must fit the SM's 228 KB of shared memory");
-constexpr int kMaxWarps = 24;
-constexpr int kMaxChunk = 32;
+constexpr int kMaxChunk = 32;        // lane c of a warp evaluates trace c of a chunk
 using namespace dev;
 
 // Bound of one wait for a chunk's bulk copy.  A copy of a chunk takes
@@ -89,25 +89,23 @@ struct ChunkSync {
     unsigned long long bar[2];
     int stalled;
 };
-static_assert(sizeof(ColInfo) * kMaxWarps + sizeof(ChunkSync) + sizeof(FastArgs) + sizeof(int) <= 1024,
+static_assert(sizeof(ChunkSync) + sizeof(FastArgs) + sizeof(int) <= 1024,
               "static shared memory of the fast kernels within the 1 KB allowance");
 
 struct ChunkSmem {
     // layout of one CTA's dynamic shared memory
-    size_t rawBytes, crdOff, geoOff, wtabOff, total;
+    size_t rawBytes, crdOff, wtabOff, total;
 };
 
 // table: the kernel interpolates sqrt(j dt) from a per-CTA table (the table weight);
 // the prefolded and sqrt.approx weights need none, and their chunks grow by its size
-template <int W>
 __host__ __device__ __forceinline__ ChunkSmem chunk_layout(int chunk, int pitch, int esize, int nt,
                                                            bool table)
 {
     ChunkSmem L;
     L.rawBytes = (size_t)chunk * pitch * esize;              // one buffer
     L.crdOff = 2 * L.rawBytes;                               // [2][5][chunk] floats
-    L.geoOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
-    L.wtabOff = L.geoOff + (size_t)chunk * W * sizeof(float4);
+    L.wtabOff = L.crdOff + ((2 * 5 * (size_t)chunk * 4 + 15) / 16) * 16;
     L.total = L.wtabOff + (table ? (size_t)(nt + 1) * sizeof(float2) : 0);   // [nt+1] weight table
     return L;
 }
@@ -133,15 +131,14 @@ enum { kOutImage = 0, kOutPartial = 1, kOutAtomic = 2 };
 template <class SH, int R, int PICK, int FMT, int PRE, int GRAD>
 __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colGroup, int runIdx,
                                           int kb, int ke, float* __restrict__ partial, int outMode,
-                                          unsigned char* smem_raw, ColInfo* cinfo, ChunkSync& cs)
+                                          unsigned char* smem_raw, ChunkSync& cs)
 {
     static_assert(R % 2 == 0, "R pairs");
     using T = typename Elem<FMT>::T;
     const Geometry& g = a.g;
-    const ChunkSmem L = chunk_layout<SH::kWarps>(chunk, a.pitch, sizeof(T), a.g.nt, PRE == kWtTable);
+    const ChunkSmem L = chunk_layout(chunk, a.pitch, sizeof(T), a.g.nt, PRE == kWtTable);
     T* rawBase = reinterpret_cast<T*>(smem_raw);
     float* crdBase = reinterpret_cast<float*>(smem_raw + L.crdOff);
-    float4* geo = reinterpret_cast<float4*>(smem_raw + L.geoOff);
     float2* wtab = reinterpret_cast<float2*>(smem_raw + L.wtabOff);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -181,12 +178,7 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
         smin = fminf(smin, __shfl_xor_sync(0xffffffffu, smin, o));
         nvalid += __shfl_xor_sync(0xffffffffu, nvalid, o);
     }
-    if (lane == 0) {
-        cinfo[warp].x = g.x0 + (float)ci * g.dx;
-        cinfo[warp].y = g.y0 + (float)cj * g.dy;
-        cinfo[warp].t2min = t2min;
-        cinfo[warp].smin = colValid ? smin : -1.0f;
-    }
+    const float colX = g.x0 + (float)ci * g.dx, colY = g.y0 + (float)cj * g.dy;
     if (PRE == kWtTable) {
         for (int j = threadIdx.x; j <= g.nt; j += SH::kThreads) {
             const float w0 = sqrtf((float)j * g.dt), w1 = sqrtf((float)(j + 1) * g.dt);
@@ -238,44 +230,42 @@ __device__ __forceinline__ bool fast_tile(const FastArgs& a, int chunk, int colG
         __syncthreads();                       // chunk ch landed; chunk ch-1 fully consumed
         if (cs.stalled) return false;          // CTA-uniform: no output from this tile
         if (ch + 1 < nchunks) issue(ch + 1);
-        // ---- per (trace, column) distances, scale and skip flag --------------
-        {
-            const float* crd = crdBase + b * 5 * chunk;
-            for (int p = threadIdx.x; p < chunk * SH::kWarps; p += SH::kThreads) {
-                const int c = p / SH::kWarps, w = p % SH::kWarps;
-                float4 gd = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
-                const ColInfo cw = cinfo[w];
-                if (c < n && cw.smin >= 0.0f) {
-                    const float mx = crd[c], my = crd[chunk + c], ox = crd[2 * chunk + c],
-                                oy = crd[3 * chunk + c], sc = crd[4 * chunk + c];
-                    const float dmx = mx - cw.x, dmy = my - cw.y;
-                    const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
-                    const float ds = sx * sx + sy * sy, dr = rx * rx + ry * ry;
-                    bool keep = !(ap2 >= 0.0f && dmx * dmx + dmy * dmy > ap2);
-                    if (keep) {
-                        // lower bound of u over the run: past the last sample -> no contribution
-                        // approximate square roots: the margin below covers their error
-                        const float ulb = sqrt_approx(fmaf(ds, cw.smin, cw.t2min)) +
-                                          sqrt_approx(fmaf(dr, cw.smin, cw.t2min));
-                        keep = ulb < umax * 1.0001f + 1.0f;
-                    }
-                    if (keep) gd = make_float4(ds, dr, sc, 0.0f);
-                }
-                geo[p] = gd;
-            }
-        }
-        __syncthreads();
         if (colValid) {
+            // ---- lane c: trace c's distances, scale and skip flag for this column ----
+            // (chunk <= 32); the warp then walks the kept traces in increasing c,
+            // taking their values by shuffle: no shared table, no second barrier
+            const float* crd = crdBase + b * 5 * chunk;
+            float lds_ = 0.0f, ldr_ = 0.0f, lsc = 0.0f;
+            bool keep = false;
+            if (lane < n) {
+                const float mx = crd[lane], my = crd[chunk + lane], ox = crd[2 * chunk + lane],
+                            oy = crd[3 * chunk + lane];
+                lsc = crd[4 * chunk + lane];
+                const float dmx = mx - colX, dmy = my - colY;
+                const float sx = dmx - ox, sy = dmy - oy, rx = dmx + ox, ry = dmy + oy;
+                lds_ = fmaf(sx, sx, sy * sy);           // explicit fusions: the same
+                ldr_ = fmaf(rx, rx, ry * ry);           // values in every build
+                keep = !(ap2 >= 0.0f && fmaf(dmx, dmx, dmy * dmy) > ap2);
+                if (keep) {
+                    // lower bound of u over the run: past the last sample -> no contribution
+                    // approximate square roots: the margin below covers their error
+                    const float ulb = sqrt_approx(fmaf(lds_, smin, t2min)) +
+                                      sqrt_approx(fmaf(ldr_, smin, t2min));
+                    keep = ulb < umax * 1.0001f + 1.0f;
+                }
+            }
             const unsigned rowsS = smem_u32(reinterpret_cast<const unsigned char*>(rawBase) + b * L.rawBytes);
             // bits(fl) = kMagicBits + i0: fold the magic offset into the bases (mod 2^32)
             const unsigned magicT = (unsigned)kMagicBits * (unsigned)sizeof(T);
             const unsigned wS = smem_u32(wtab) - (unsigned)kMagicBits * 8u;
-            for (int c = 0; c < n; c++) {
-                const float4 gd = geo[c * SH::kWarps + warp];
-                if (gd.x < 0.0f) continue;                 // warp-uniform
+            for (unsigned kept = __ballot_sync(0xffffffffu, keep); kept; kept &= kept - 1u) {
+                const int c = __ffs(kept) - 1;
+                const float ds = __shfl_sync(0xffffffffu, lds_, c);
+                const float dr = __shfl_sync(0xffffffffu, ldr_, c);
+                const float sc = __shfl_sync(0xffffffffu, lsc, c);
                 keptTraces++;
                 const unsigned rowS = rowsS + (unsigned)(c * a.pitch) * (unsigned)sizeof(T) - magicT;
-                const f2 DS = pk(gd.x, gd.x), DR = pk(gd.y, gd.y), SC = pk(gd.z, gd.z);
+                const f2 DS = pk(ds, ds), DR = pk(dr, dr), SC = pk(sc, sc);
 #pragma unroll
                 for (int h = 0; h < R / 2; h++) {
                     if (GRAD) {
@@ -394,7 +384,6 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
              const BatchTile* __restrict__ tiles, int ntiles, unsigned* __restrict__ counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ ColInfo cinfo[SH::kWarps];
     __shared__ ChunkSync cs;
     __shared__ FastArgs sa;
     __shared__ int st;
@@ -410,7 +399,7 @@ batch_kernel(const FastArgs* __restrict__ jobs, const int* __restrict__ chunks,
         for (int i = threadIdx.x; i < (int)(sizeof(FastArgs) / 4); i += SH::kThreads) dst[i] = src[i];
         __syncthreads();
         const bool ok = fast_tile<SH, R, PICK, FMT, PRE, 0>(sa, chunks[tl.job], tl.cg, tl.run, tl.kb, tl.ke,
-                                                        nullptr, kOutAtomic, smem_raw, cinfo, cs);
+                                                        nullptr, kOutAtomic, smem_raw, cs);
         __syncthreads();                           // shared memory is reused by the next tile
         if (!ok) break;                            // CTA-uniform
     }
@@ -421,14 +410,13 @@ __global__ void __launch_bounds__(SH::kThreads, SH::kMinBlocks)
 fast_kernel(FastArgs a, int chunk, int perSlice, float* __restrict__ partial)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ ColInfo cinfo[SH::kWarps];
     __shared__ ChunkSync cs;
     const int kb = blockIdx.z * perSlice;
     const int ke = min(a.g.ntr, kb + perSlice);
     const size_t nimg = (size_t)a.g.nx * a.g.ny * a.g.nz;
     fast_tile<SH, R, PICK, FMT, PRE, GRAD>(a, chunk, blockIdx.x, blockIdx.y, kb, ke,
                                        partial ? partial + blockIdx.z * nimg : nullptr,
-                                       partial ? kOutPartial : kOutImage, smem_raw, cinfo, cs);
+                                       partial ? kOutPartial : kOutImage, smem_raw, cs);
 }
 
 // out[i] = (accumulate ? out[i] : 0) + sum_z partial[z][i], z in increasing order
@@ -451,9 +439,9 @@ int fast_chunk(const FastArgs& a, int esize, bool table)
 {
     int chunk = kMaxChunk;
     if (a.chunkCap > 0) chunk = std::min(chunk, a.chunkCap);
-    while (chunk > 1 && chunk_layout<SH::kWarps>(chunk, a.pitch, esize, a.g.nt, table).total > SH::kBudget)
+    while (chunk > 1 && chunk_layout(chunk, a.pitch, esize, a.g.nt, table).total > SH::kBudget)
         chunk--;
-    if (chunk_layout<SH::kWarps>(chunk, a.pitch, esize, a.g.nt, table).total > (size_t)kMaxSmemBytes)
+    if (chunk_layout(chunk, a.pitch, esize, a.g.nt, table).total > (size_t)kMaxSmemBytes)
         return 0;
     return chunk;
 }
@@ -469,7 +457,7 @@ int launch_block(const FastArgs& a, cudaStream_t stream, int smCount)
     if (chunk == 0)
         return set_error(KTM_ERR_LIMIT, "fast kernel: packed pitch %d exceeds the shared-memory "
                                         "stage limit", a.pitch);
-    const size_t smem = chunk_layout<SH::kWarps>(chunk, a.pitch, esize, g.nt, kTable).total;
+    const size_t smem = chunk_layout(chunk, a.pitch, esize, g.nt, kTable).total;
     auto kern = fast_kernel<SH, R, PICK, FMT, PRE, GRAD>;
     KTM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
@@ -747,7 +735,7 @@ int launch_batch_t(const FastArgs* jobs, int njobs, cudaStream_t s)
         if (c == 0)
             return set_error(KTM_ERR_LIMIT, "batch: job %d packed pitch %d exceeds shared memory", j,
                              jobs[j].pitch);
-        const size_t need = chunk_layout<SH::kWarps>(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total;
+        const size_t need = chunk_layout(c, jobs[j].pitch, esize, g.nt, PRE == kWtTable).total;
         chunks[j] = c;
         smem = std::max(smem, need);
         totalPairs += (double)g.nx * g.ny * g.nz * g.ntr;

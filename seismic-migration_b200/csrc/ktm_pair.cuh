@@ -215,12 +215,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     }
 }
 
-struct ColInfo {
-    float x, y;       // column coordinates
-    float t2min;      // min over the run of (tau/dt)^2
-    float smin;       // min over the run of S' = 1/(v dt)^2; < 0: column outside the image
-};
-
 
 // Kinematics of two pairs (tau samples r and r+1 of one lane) with one trace:
 //   a_s = T2' + Ds S', a_r = T2' + Dr S'   (sample units)
