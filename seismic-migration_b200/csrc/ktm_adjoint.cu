@@ -286,7 +286,9 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
     if (!accumulate && g.ntr > 0)
         KTM_CUDA_TRY(cudaMemsetAsync(data, 0, pitchBytes * g.ntr, s));
     if (g.ntr == 0 || (long long)g.nx * g.ny * g.nz == 0) return KTM_OK;
-    const size_t fixed = (size_t)padded_pitch(g.nt + 1) * sizeof(float2) + 64;
+    const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : weightMethod == KTM_WEIGHT_PREFOLD ? 2 : 0;
+    // the sqrt(j dt) table only for the table weight; the coordinates' alignment pad
+    const size_t fixed = (wt == 0 ? (size_t)padded_pitch(g.nt + 1) * sizeof(float2) : 0) + 64;
     const size_t perTrace = (size_t)padded_pitch(pitch) * sizeof(float) + 4 * sizeof(float);
     int chunk = 32;                     // at most 32: lane c evaluates trace c's geometry
     while (chunk > 1 && fixed + chunk * perTrace > kAdjSmemBudget) chunk--;
@@ -319,7 +321,6 @@ int launch_demigrate(const Geometry& g, const float* midX, const float* midY, co
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
         demigrate_merge_kernel<P, W><<<grid, kAdjThreads, smem, s>>>(a);                       \
     } while (0)
-    const int wt = weightMethod == KTM_WEIGHT_SQRT ? 1 : weightMethod == KTM_WEIGHT_PREFOLD ? 2 : 0;
     if (wt == 2 && pick != KTM_PICK_LINEAR)
         return set_error(KTM_ERR_ARG, "demigrate: the prefolded weight takes the linear pick");
     if (pick == KTM_PICK_LINEAR) {

@@ -1,6 +1,7 @@
 """Demigration (the adjoint), the Vrms gradient and least-squares migration.
 
-* demigration against the FP64 oracle's transpose (same formulation);
+* demigration against the FP64 oracle's transpose (same formulation), also with
+  6000-sample traces and a coarse tau step;
 * dot-product tests <L m, d> = <m, L^T d> to 1e-5 (seeded Gaussian m and d),
   including the 512 CMP x 64 offset x 1001 sample line of the adjoint/LSM
   configuration;
@@ -58,6 +59,26 @@ def test_demigrate_matches_oracle_transpose(cuda, ktm_lib, pick, weight):
     # at FP32 rounding of t/dt move a white-noise model's contributions one sample
     tol = 5e-5 if pick == "linear" else 1e-2
     assert rel_l2(d[:, :sv.nt], ref) < tol
+
+
+@pytest.mark.parametrize("weight", ["table", "prefold"])
+def test_demigrate_long_traces_coarse_tau(cuda, ktm_lib, weight):
+    """6000-sample traces (padded accumulator rows of ~30 KB: a few traces per chunk)
+    and a tau step of 1.25 dt, so t/dt moves on by two or more samples between a lane's
+    consecutive tau samples (the merge flushes both samples of its pick) -- against the
+    FP64 oracle's transpose."""
+    sv, op = line_op(cuda, ncmp=16, noff=4, nt=6000, nz=300, aperture=400.0, weight=weight,
+                     dtau=0.005)
+    m = np.random.default_rng(2).standard_normal(op.shape).astype(np.float32)
+    d = op.demigrate(_t(m, cuda)).cpu().numpy()
+    ref = oracle.demigrate_f64(sv.imageX, sv.imageY, sv.imageZ, sv.dt, sv.midX, sv.midY, sv.offX,
+                               sv.offY, sv.nt, sv.velocity, m, pick=1, aperture=400.0,
+                               prefold=1 if weight == "prefold" else 3)
+    assert np.abs(ref).max() > 0
+    assert not d[:, 0].any() and not d[:, sv.nt:].any()
+    # t/dt reaches ~750 samples here, where the FP32 square roots move f by ~1e-4 of a
+    # sample, and each data sample sums fewer contributions than on the finer tau grid
+    assert rel_l2(d[:, :sv.nt], ref) < 1e-4
 
 
 @pytest.mark.parametrize("pick,weight,aperture", [("linear", "table", 0.0), ("linear", "table", 300.0),
