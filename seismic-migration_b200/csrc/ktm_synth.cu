@@ -3,7 +3,9 @@
 // double-square-root time source -> scatterer -> receiver, plus N(0, sigma)
 // noise from a counter hash (splitmix64 of seed*2^48 + k*2^22 + j, two 32-bit
 // halves through Box-Muller).  FP64 arithmetic, so the device traces agree
-// with the numpy ones to float rounding.  Test and benchmark input only.
+// with the numpy ones to float rounding when both use the same (float) sample
+// interval; each sample sums the scatterers in order, so a run repeats bit for
+// bit.  Test and benchmark input only.
 #include "ktm_internal.cuh"
 
 namespace ktm {
@@ -48,8 +50,9 @@ __global__ void __launch_bounds__(256) synth_kernel(SynthArgs a)
             if (j < 0 || j >= a.nt) continue;
             const double q = pf * ((double)j * a.dt - t);
             const double e = q * q;
-            atomicAdd(&acc[j], (float)(amp * (1.0 - 2.0 * e) * exp(-e)));
+            acc[j] += (float)(amp * (1.0 - 2.0 * e) * exp(-e));   // one thread per sample
         }
+        __syncthreads();   // scatterer by scatterer: every sample sums them in order (repeatable)
     }
     __syncthreads();
     const unsigned long long kk = (unsigned long long)(a.k0 + k);
