@@ -549,7 +549,9 @@ def lsm_main(a):
     opp = MigrationOperator(velocity=cube * (1 + eps), **gkw)
     opm = MigrationOperator(velocity=cube * (1 - eps), **gkw)
     fd = (opp.migrate(packed) - opm.migrate(packed)).double() / (2 * eps * cube.double())
-    g = gop.vrms_gradient(gop.packed(packed)).double()
+    gpk = gop.packed(packed)
+    g = gop.vrms_gradient(gpk).double()
+    grad_ms = timed(lambda: gop.vrms_gradient(gpk))
     npairs = op.shape[0] * op.shape[1] * op.shape[2] * sv.ntr
     print(json.dumps({
         "metric": "adjoint / LSM, 2-D line 512 CMPs x 64 offsets x 1001 samples",
@@ -562,6 +564,8 @@ def lsm_main(a):
         "lsm_20": {"seconds": lsm_s, "residual_ratio": float(rn[-1] / rn[0]),
                    "gradient_ratio": float(gn[-1] / gn[0]), "graph": True},
         "vrms_gradient_vs_fd": {"rel_l2": float((g - fd).norm() / fd.norm()), "eps": eps},
+        "vrms_gradient_ms": grad_ms,
+        "vrms_gradient_gpair_s": npairs / (grad_ms * 1e-3) / 1e9,
     }), flush=True)
 
 
