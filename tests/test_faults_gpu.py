@@ -8,7 +8,10 @@
   reference picks most often): the NaN reaches exactly the image samples whose
   truncated pick lands on it, as in the reference's own compiled
   psktmCPU.c (oracle/_ref, one thread; the oracle restatement where it was not
-  built); every other sample stays bit-identical.
+  built); every other sample stays bit-identical;
+* reference mode, zero / negative / 1e30 / infinite / NaN velocities and infinite
+  samples: the reference's NaN and infinite image samples, through both drop-in
+  entry points.
 """
 from __future__ import annotations
 
@@ -82,3 +85,22 @@ def test_nan_sample_reaches_the_reference_picks(cuda, ktm_lib):
     assert np.array_equal(np.isnan(got), np.isnan(ref))
     fin = ~np.isnan(ref)
     assert np.array_equal(got[fin].view(np.uint32), ref[fin].view(np.uint32))
+
+
+@pytest.mark.parametrize("entry", ["ktmMigrationCPU", "ktmMigrationGPU"])
+def test_degenerate_velocity_and_samples_reference_mode(cuda, ktm_lib, entry):
+    """Zero, negative, 1e30, infinite and NaN velocities and infinite trace samples
+    through the drop-in entry points: the same NaN and infinite image samples as the
+    reference's own compiled psktmCPU.c (one thread; the oracle restatement where it
+    was not built), every other sample bit-identical."""
+    import ktm
+    from conftest import degenerate_reference_case, same_with_nans
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = degenerate_reference_case()
+    cfg = ktm.JobParams(tr.shape[0], tr.shape[1], dt)
+    got = getattr(ktm, entry)(gx, gy, gz, cfg, mx, my, ox, oy, tr, vel)
+    if oracle.ref_available():
+        ref = oracle.migrate_reference_c(gx, gy, gz, dt, mx, my, ox, oy, tr, vel, threads=1)
+    else:
+        ref = oracle.migrate_ref32(gx, gy, gz, dt, mx, my, ox, oy, tr, vel)
+    assert np.isnan(ref).any() and np.isinf(ref).any()
+    assert same_with_nans(got, ref)

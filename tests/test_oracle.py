@@ -156,3 +156,15 @@ def test_rho_octave_matrix_fftshift_rotates_odd_trace_counts():
     assert np.allclose(script, np.roll(per_trace, -1, axis=0))
     x = x[:4]
     assert np.allclose(rho.apply_rho_filter(x, 2000.0, 3), rho.rho_filter_traces(x, 2000.0, 3))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+def test_ref32_restatement_matches_reference_library_degenerate():
+    """Zero, negative, huge, infinite and NaN velocities and infinite trace samples:
+    the restatement reproduces the reference's NaN and infinite image samples."""
+    from conftest import degenerate_reference_case, same_with_nans
+    args = degenerate_reference_case()
+    a = oracle.migrate_ref32(*args)
+    b = oracle.migrate_reference_c(*args, threads=1)
+    assert np.isnan(b).any() and np.isinf(b).any() and np.isfinite(b).any()
+    assert same_with_nans(a, b)
