@@ -152,6 +152,25 @@ def test_fast_linear_matches_f64_oracle(cuda, ktm_lib, seed):
     assert rel_l2(img, ref0) < 1e-3
 
 
+def test_deep_image_and_long_traces(cuda, ktm_lib):
+    """Nz = 5000 (the reference's GPU host capped Nz at 2048) and 6000-sample traces:
+    reference mode bit-identical to the oracle restatement, fast mode (several tau runs
+    per column, the trace-end cull) against the FP64 oracle."""
+    import ktm
+    case = random_case(8, ntr=24, nt=6000, nx=2, ny=1, nz=5000)
+    gx, gy, gz, dt, mx, my, ox, oy, tr, vel = case
+    ref = oracle.migrate_ref32(*case)
+    assert np.count_nonzero(ref) > 0
+    cfg = ktm.JobParams(tr.shape[0], tr.shape[1], dt)
+    img = ktm.ktmMigrationGPU(gx, gy, gz, cfg, mx, my, ox, oy, tr, vel)
+    assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+    got = fast(cuda, case, pick="linear")
+    # t/dt reaches ~6000 samples here: sqrt.approx's ~2^-22 relative error moves a pick
+    # by up to ~1.5e-3 of a sample, which white-noise traces turn into that much
+    # relative error (2e-5 at the ~300 samples of the shallow cases above)
+    assert rel_l2(got, oracle.migrate_f64(*case, pick=1, prefold=3)) < 1e-3
+
+
 def test_fast_truncate_matches_f64_oracle(cuda, ktm_lib):
     # tau step incommensurate with dt: with dz = dt/2 every zero-offset pair has an
     # exactly integer t/dt, and FP32 rounding then truncates about half of them one
